@@ -1,0 +1,423 @@
+"""Benchmark of the GPU geodesic render path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One step renders one 1024x1024 frame of the near edge-on scene (a = 0.998,
+inclination 85 deg, disc r_isco..50 M at 0.3 Eddington, M = 10 M_sun, +-25 M
+field of view from r = 1000 M, one sample per pixel, seeded 250,000-star
+uniform sky): 1,048,576 rays, traced in mixed precision.  The same frame in
+plain FP64 is timed beside it, and the per-pixel error of the mixed frame
+against the FP64 frame is reported.
+
+Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events on
+the stream the kernels run on, with a 256 MiB write between steps to flush the
+126 MB L2; barrier + synchronize around the timed loop; the maximum over ranks
+is reported.  Under torchrun each rank renders its own frame (camera azimuth
+2 pi rank / N): weak scaling with no collective on the data path.
+
+`--impl reference` times the reference's own CPU implementation (the
+reference renderer compiled from its sources, oracle/_ref) on the box's host
+cores, on rows of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "rays/s at 1024² on 1 B200: mixed vs FP64 plain at stated g/dir error; grads/s"
+WORKLOAD = ("edge_on_1024: a=0.998, inclination 85 deg, 1024x1024, 1 spp, +-25 M from r=1000 M, "
+            "disc r_isco..50 M at 0.3 Eddington, M=10 M_sun, 250k-star uniform sky + 21.5 mag/arcsec^2 "
+            "background, escape 1.1 r_obs, horizon stop r_+(1+1e-6), rtol 1e-8 / atol 1e-10 (FP64), "
+            "1e-6 / 1e-8 (mixed)")
+L2_FLUSH_BYTES = 256 << 20
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "trace_kernel_traffic.txt")
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    p.add_argument("--size", type=int, default=1024, help="frame side (default 1024)")
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def frame_config(size: int, rank: int, world: int, precision: int):
+    from blackhole_b200 import workloads
+
+    cfg = workloads.edge_on_1024(precision=precision)
+    cfg.width = cfg.height = size
+    cfg.cam.phi = 2.0 * math.pi * rank / max(1, world)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------
+
+def time_device(r, cfg, steps, warmup, torch, flush, barrier):
+    """Average device time of one render (CUDA events on the render stream)."""
+    from blackhole_b200 import abi
+
+    stream = torch.cuda.current_stream()
+    dev = torch.empty((cfg.height, cfg.width, 3), dtype=torch.float64, device="cuda")
+    c = cfg.to_c()
+    for _ in range(warmup):
+        r.render_device(c, dev.data_ptr(), stream.cuda_stream)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    barrier()
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush.add_(1.0)
+        starts[i].record(stream)
+        r.render_device(c, dev.data_ptr(), stream.cuda_stream)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    times = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    st = abi.bh_render_stats()
+    r.render_device(c, dev.data_ptr(), stream.cuda_stream, stats=st)
+    return sum(times), times, st, dev
+
+
+def roofline(kernel_ms: float, steps: int, attempts: int, precision: str, peak: float, peak_src: str):
+    from blackhole_b200 import flops
+
+    per = flops.FLOPS_PER_STEP[precision]
+    algo = per["alu_flop"] * steps          # accepted steps are the unit of work
+    achieved = algo / (kernel_ms * 1e-3) / 1e12
+    traffic = None
+    if os.path.exists(PROFILE_TRAFFIC):
+        for ln in open(PROFILE_TRAFFIC):
+            if ln.startswith(f"{precision}_bytes_per_launch:"):
+                try:
+                    traffic = float(ln.split(":", 1)[1].strip())
+                except ValueError:
+                    pass
+    return {
+        "bound": "fp32-alu" if precision == "mixed" else "fp64-alu",
+        "achieved": round(achieved, 3),
+        "peak": round(peak, 3),
+        "unit": "TFLOP/s",
+        "frac": round(achieved / peak, 4) if peak > 0 else None,
+        "traffic": traffic,
+        "peak_source": peak_src,
+        "flop_per_step": per["alu_flop"],
+        "f64_flop_per_step": per["f64_flop"],
+        "accepted_steps": steps,
+        "attempts": attempts,
+        "kernel_ms": round(kernel_ms, 4),
+    }
+
+
+def accuracy(r, size, rank, world):
+    """Per-ray error of the mixed frame against the FP64 frame (same rays)."""
+    from blackhole_b200 import abi
+
+    a = r.trace_rays(frame_config(size, rank, world, abi.PRECISION_FP64))
+    b = r.trace_rays(frame_config(size, rank, world, abi.PRECISION_MIXED))
+    same = a["what"] == b["what"]
+    out = {"class_agree": float(same.mean()), "against": "the FP64 GPU frame (per ray)"}
+    disc = same & (a["what"] == abi.HIT_DISC) & (a["g"] > 0)
+    if disc.any():
+        e = np.abs(b["g"][disc] - a["g"][disc]) / a["g"][disc]
+        out["g_rel"] = {"p50": float(np.quantile(e, .5)), "p99": float(np.quantile(e, .99)),
+                        "max": float(e.max()), "frac_le_1e-3": float((e <= 1e-3).mean()), "n": int(disc.sum())}
+    sky = same & (a["what"] == abi.HIT_SKY)
+    if sky.any():
+        d = 2 * np.arcsin(np.clip(np.linalg.norm(b["dir"][sky] - a["dir"][sky], axis=1) / 2, 0, 1))
+        out["dir_rad"] = {"p50": float(np.quantile(d, .5)), "p99": float(np.quantile(d, .99)),
+                          "max": float(d.max()), "frac_le_1e-4": float((d <= 1e-4).mean()), "n": int(sky.sum())}
+    return out
+
+
+def cpu_baseline(size: int, max_seconds: float = 20.0):
+    """The reference CPU path on a bounded sample of the frame's rows."""
+    import oracle
+    from blackhole_b200 import abi
+
+    cfg = frame_config(size, 0, 1, abi.PRECISION_FP64)
+    ref = oracle.reference()
+    threads = os.cpu_count() or 1
+    if ref is not None:
+        # The reference has one sky and one stop rule: run its own.
+        cfg.sky_mode = abi.SKY_GALACTIC
+        cfg.stop_mode = abi.STOP_REFERENCE
+        rows = list(range(0, cfg.height, 16))
+        t0 = time.perf_counter()
+        _, st, setup = ref.render_rows(cfg, rows, threads)
+        wall = time.perf_counter() - t0 - setup
+        return {"value": st.rays / st.seconds, "unit": "rays/s", "cores": threads, "kind": "reference",
+                "sample": f"{len(rows)} of {cfg.height} rows ({st.rays} rays) of the {size}x{size} frame, "
+                          f"reference sky and horizon stop (its only ones), trace+shade on {threads} threads, "
+                          f"{st.seconds:.2f} s excluding {setup:.2f} s scene set-up",
+                "seconds": st.seconds}
+    port = oracle.oracle()
+    w = 64
+    t0 = time.perf_counter()
+    _, st = port.trace_rays(cfg, (size - w) // 2, (size - w) // 2, w, 8)
+    dt = time.perf_counter() - t0
+    return {"value": st.rays / dt, "unit": "rays/s", "cores": 1, "kind": "port",
+            "sample": f"{st.rays} rays of a {w}x8 window at the frame centre, oracle port, 1 thread",
+            "seconds": dt}
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    from blackhole_b200 import Renderer, abi, gpu
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    r = Renderer(local)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    size = args.size
+    cfg_m = frame_config(size, rank, world, abi.PRECISION_MIXED)
+    rays = cfg_m.n_rays
+
+    with ClockSampler(local) as clk:
+        t_mixed, times_m, st_m, _ = time_device(r, cfg_m, args.steps, args.warmup, torch, flush, barrier)
+    t_mixed = max_over_ranks(t_mixed)
+    value = world * rays * args.steps / (t_mixed * 1e-3)
+
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "rays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_mixed / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 state/stages + f64 Delta/Sigma/error-norm/roots/diagnostics",
+        "data": "synthetic (seeded camera rays and star catalogue)",
+        "config": {"workload": WORKLOAD, "precision": "mixed", "rays_per_step": rays, "frame": f"{size}x{size}",
+                   "partition": "one frame per GPU, camera azimuth 2 pi rank/N",
+                   "l2": "256 MiB write between timed steps (L2 flushed)"},
+    }
+
+    # FP64 plain path, same frame.
+    if not args.no_fp64:
+        cfg_d = frame_config(size, rank, world, abi.PRECISION_FP64)
+        t_fp64, _, st_d, _ = time_device(r, cfg_d, max(2, args.steps // 2), 1, torch, flush, barrier)
+        t_fp64 = max_over_ranks(t_fp64)
+        v64 = world * rays * max(2, args.steps // 2) / (t_fp64 * 1e-3)
+        out["fp64"] = {"value": round(v64, 1), "unit": "rays/s",
+                       "ms_per_step": round(t_fp64 / max(2, args.steps // 2), 4),
+                       "steps_per_ray": round(st_d.steps / st_d.rays, 2),
+                       "attempts_per_ray": round(st_d.attempts / st_d.rays, 2)}
+        out["mixed_over_fp64"] = round(value / v64, 3)
+
+    out["steps_per_ray"] = round(st_m.steps / st_m.rays, 2)
+    out["attempts_per_ray"] = round(st_m.attempts / st_m.rays, 2)
+    out["classes"] = {"captured": st_m.captured, "disc": st_m.disc_hits, "sky": st_m.escaped,
+                      "exhausted": st_m.exhausted}
+    out["diagnostics"] = {"max_norm_error": st_m.max_norm_error, "max_carter_drift": st_m.max_carter_drift}
+
+    # Roofline of the dominant kernel (the trace kernel).
+    peak32 = gpu.fma_peak_tflops(local, abi.PRECISION_MIXED)
+    peak64 = gpu.fma_peak_tflops(local, abi.PRECISION_FP64)
+    out["roofline"] = roofline(st_m.kernel_ms, st_m.steps, st_m.attempts, "mixed", peak32,
+                               "FP32 FMA throughput measured in this run (bh_gpu_fma_peak)")
+    if "fp64" in out:
+        out["fp64"]["roofline"] = roofline(st_d.kernel_ms, st_d.steps, st_d.attempts, "fp64", peak64,
+                                           "FP64 FMA throughput measured in this run (bh_gpu_fma_peak)")
+    out["kernel_share"] = {"trace_ms": round(st_m.kernel_ms, 4), "shade_ms": round(st_m.shade_ms, 4)}
+
+    if rank == 0:
+        try:
+            out["accuracy"] = accuracy(r, size, rank, world)
+        except Exception as e:  # reported, not hidden
+            out["accuracy"] = {"error": repr(e)}
+
+    # End to end through the public API: host output buffer, synchronous call.
+    from blackhole_b200 import RenderStats
+
+    host = torch.empty((size, size, 3), dtype=torch.float64, pin_memory=True).numpy()
+    st_e = RenderStats()
+    for _ in range(max(1, args.warmup)):
+        r.render_into(cfg_m, host)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s = abi.bh_render_stats()
+        r.render_into(cfg_m, host, s)
+        st_e.h2d_bytes, st_e.d2h_bytes = s.h2d_bytes, s.d2h_bytes
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    out["e2e"] = {"value": round(world * rays * args.steps / t_e2e, 1), "unit": "rays/s",
+                  "h2d_bytes_per_step": int(st_e.h2d_bytes), "d2h_bytes_per_step": int(st_e.d2h_bytes),
+                  "api": "bh_gpu_render (C-ABI) into pinned host memory, wall clock"}
+
+    # Kernels of ours launched in the timed region: trace, shade, 2 reduce per step.
+    out["gpu_launches"] = 4 * args.steps
+    out["clocks"] = clk.summary()
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(size)
+        except Exception as e:
+            out["cpu_baseline"] = {"value": None, "error": repr(e)}
+
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    r.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    from blackhole_b200 import abi
+
+    cfg = frame_config(args.size, 0, 1, abi.PRECISION_FP64)
+    ref = oracle.reference()
+    threads = os.cpu_count() or 1
+    kind = "reference"
+    if ref is None:
+        kind = "port"
+        threads = 1
+    else:
+        cfg.sky_mode = abi.SKY_GALACTIC
+        cfg.stop_mode = abi.STOP_REFERENCE
+    # Each step: a bounded sample of rows (disjoint row sets cycle through the frame).
+    rows_per_step = 16
+    stride = max(1, cfg.height // rows_per_step)
+
+    def step(i):
+        rows = [(k * stride + i * 7) % cfg.height for k in range(rows_per_step)]
+        if ref is not None:
+            _, st, _ = ref.render_rows(cfg, rows, threads)
+            return st.rays, st.seconds
+        port = oracle.oracle()
+        t0 = time.perf_counter()
+        _, st = port.trace_rays(cfg, 0, rows[0], cfg.width, 1)
+        return st.rays, time.perf_counter() - t0
+
+    for i in range(args.warmup):
+        step(i)
+    n, secs = 0, 0.0
+    for i in range(args.steps):
+        a, b = step(args.warmup + i)
+        n += a
+        secs += b
+    value = n / secs
+    sample = (f"{rows_per_step} rows of the {args.size}x{args.size} frame per step "
+              f"({rows_per_step * cfg.width} rays), reference sky and horizon stop (its only ones)"
+              if ref is not None else f"one row of the frame per step, oracle port")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "rays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * secs / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded camera rays and star catalogue)",
+        "config": {"workload": WORKLOAD, "precision": "fp64 (the reference's only)", "frame": f"{args.size}x{args.size}"},
+        "cpu_baseline": {"value": round(value, 1), "unit": "rays/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": round(value, 1), "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

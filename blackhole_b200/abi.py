@@ -1,0 +1,147 @@
+"""ctypes mirror of include/bh_gpu.h.
+
+The field order and types here must match the C header exactly; the
+library checks ``struct_size`` and ``abi_version`` on every call, and
+tests/test_abi.py compares these layouts against the compiled header.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+ABI_VERSION = 1
+
+# Status codes (bh_gpu.h).
+OK = 0
+ERR_INVALID_ARG = -1
+ERR_CUDA = -2
+ERR_BUDGET = -3
+ERR_ABORTED = -4
+ERR_NO_DEVICE = -5
+ERR_UNSUPPORTED = -6
+ERR_OUT_OF_MEMORY = -7
+
+STATUS_NAMES = {
+    OK: "BH_OK",
+    ERR_INVALID_ARG: "BH_ERR_INVALID_ARG",
+    ERR_CUDA: "BH_ERR_CUDA",
+    ERR_BUDGET: "BH_ERR_BUDGET",
+    ERR_ABORTED: "BH_ERR_ABORTED",
+    ERR_NO_DEVICE: "BH_ERR_NO_DEVICE",
+    ERR_UNSUPPORTED: "BH_ERR_UNSUPPORTED",
+    ERR_OUT_OF_MEMORY: "BH_ERR_OUT_OF_MEMORY",
+}
+
+# Termination classes, in the order of Hit::What (render.cpp:37).
+HIT_HORIZON, HIT_DISC, HIT_SUN, HIT_STAR, HIT_SKY, HIT_EXHAUSTED = range(6)
+HIT_NAMES = ("Horizon", "Disc", "Sun", "Star", "Sky", "Exhausted")
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+SKY_GALACTIC = 0
+SKY_UNIFORM = 1
+STOP_REFERENCE = 0
+STOP_RELATIVE = 1
+
+
+class bh_xyz(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+class bh_camera(C.Structure):
+    _fields_ = [
+        ("r", C.c_double), ("theta", C.c_double), ("phi", C.c_double),
+        ("fov", C.c_double), ("yaw", C.c_double), ("pitch", C.c_double), ("roll", C.c_double),
+    ]
+
+
+class bh_sun(C.Structure):
+    _fields_ = [("centre", C.c_double * 3), ("radius", C.c_double), ("T_eff", C.c_double)]
+
+
+class bh_hotspot(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_int32), ("sense", C.c_int32),
+        ("r", C.c_double), ("phi0", C.c_double), ("sigma", C.c_double),
+        ("contrast", C.c_double), ("omega", C.c_double),
+    ]
+
+
+class bh_neutron_star(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_int32), ("caps", C.c_int32),
+        ("M_kg", C.c_double), ("R_m", C.c_double), ("R", C.c_double),
+        ("T_eff", C.c_double), ("spin_hz", C.c_double), ("Omega", C.c_double),
+        ("cap_tilt", C.c_double), ("cap_radius", C.c_double), ("cap_T", C.c_double),
+        ("cap_phase0", C.c_double),
+        ("two_caps", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
+class bh_render_config(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("abi_version", C.c_uint32),
+        ("M_kg", C.c_double), ("spin", C.c_double),
+        ("cam", bh_camera),
+        ("width", C.c_int32), ("height", C.c_int32), ("sqrt_spp", C.c_int32),
+        ("disc_enabled", C.c_int32),
+        ("disc_r_out", C.c_double), ("eddington", C.c_double),
+        ("disc_sense", C.c_int32), ("stars_enabled", C.c_int32),
+        ("star_count", C.c_int32), ("sun_enabled", C.c_int32),
+        ("seed", C.c_uint64),
+        ("sun", bh_sun),
+        ("hotspot", bh_hotspot),
+        ("star", bh_neutron_star),
+        ("jet_enabled", C.c_int32), ("reserved0", C.c_int32),
+        ("observer_time", C.c_double),
+        ("rtol", C.c_double), ("atol", C.c_double), ("r_escape", C.c_double),
+        ("max_steps", C.c_int32),
+        ("threads", C.c_int32), ("quiet", C.c_int32),
+        ("precision", C.c_int32), ("sky_mode", C.c_int32), ("stop_mode", C.c_int32),
+        ("milky_way", C.c_int32),
+        ("stop_epsilon", C.c_double),
+        ("mixed_rtol", C.c_double), ("mixed_atol", C.c_double),
+    ]
+
+
+class bh_render_stats(C.Structure):
+    _fields_ = [
+        ("rays", C.c_longlong), ("steps", C.c_longlong), ("captured", C.c_longlong),
+        ("disc_hits", C.c_longlong), ("sun_hits", C.c_longlong), ("star_hits", C.c_longlong),
+        ("jet_rays", C.c_longlong), ("escaped", C.c_longlong), ("exhausted", C.c_longlong),
+        ("max_norm_error", C.c_double), ("max_carter_drift", C.c_double),
+        ("seconds", C.c_double), ("total_flux", C.c_double),
+        ("attempts", C.c_longlong), ("kernel_ms", C.c_double), ("shade_ms", C.c_double),
+        ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class bh_ray_result(C.Structure):
+    _fields_ = [
+        ("what", C.c_int32), ("steps", C.c_int32),
+        ("y", C.c_double * 8), ("g", C.c_double), ("dir", C.c_double * 3),
+        ("xyz", bh_xyz),
+    ]
+
+
+class bh_launch_params(C.Structure):
+    _fields_ = [
+        ("block_size", C.c_int32), ("rays_per_thread", C.c_int32),
+        ("refill", C.c_int32), ("blocks_per_sm", C.c_int32),
+    ]
+
+
+# numpy dtype of bh_ray_result, for zero-copy views of result arrays.
+def ray_result_dtype():
+    import numpy as np
+
+    return np.dtype(
+        {
+            "names": ["what", "steps", "y", "g", "dir", "xyz"],
+            "formats": [np.int32, np.int32, (np.float64, 8), np.float64, (np.float64, 3), (np.float64, 3)],
+            "offsets": [0, 4, 8, 72, 80, 104],
+            "itemsize": C.sizeof(bh_ray_result),
+        }
+    )

@@ -1,0 +1,565 @@
+// bh_capi.cpp - The C-ABI of include/bh_gpu.h.
+//
+// A bh_ctx owns one CUDA stream on one device, the device copies of the
+// blackbody table and of the star catalogue (rebuilt only when count, seed or
+// sky mode change), and grow-only ray/pixel buffers.  A render call is: frame
+// constants -> H2D, queue reset, the persistent trace kernel, the shade
+// kernel, the stats reduction, D2H of pixels and stats.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bh_gpu.h"
+#include "bh_frame.h"
+#include "bh_launch.h"
+#include "bh_scene.h"
+
+using namespace bhg;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace
+
+struct bh_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t abort_stream = nullptr;
+    std::string err;
+    bh_launch_params launch{128, 1, 16, 0};
+    unsigned long long budget = 0;
+    std::atomic<int> abort_requested{0};
+    int32_t* h_one = nullptr;          // pinned 1, source of the abort copy
+
+    std::vector<double> h_table;
+    double* d_table = nullptr;
+
+    bool sky_valid = false;
+    int sky_count = -1;
+    uint64_t sky_seed = 0;
+    int sky_mode = -1;
+    double4* d_star_pos = nullptr;
+    double4* d_star_col = nullptr;
+    int32_t* d_bin_start = nullptr;
+    HostSky sky_meta;
+
+    DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats;
+    QueueState* d_queue = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long h2d = 0, d2h = 0;          // bytes copied by the current call
+};
+
+namespace {
+
+constexpr int kReduceBlocks = 64;
+
+int fail(bh_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(bh_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, e == cudaErrorMemoryAllocation ? BH_ERR_OUT_OF_MEMORY : BH_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                          \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+int ensure(bh_ctx* ctx, DevBuf& b, size_t bytes) {
+    if (bytes <= b.cap) return BH_OK;
+    if (b.p) {
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    const size_t want = std::max<size_t>(bytes, 256);
+    CK(cudaMalloc(&b.p, want));
+    b.cap = want;
+    return BH_OK;
+}
+
+int check_cfg_header(bh_ctx* ctx, const bh_render_config* cfg) {
+    if (!cfg) return fail(ctx, BH_ERR_INVALID_ARG, "config is NULL");
+    if (cfg->struct_size != sizeof(bh_render_config))
+        return fail(ctx, BH_ERR_INVALID_ARG, "bh_render_config.struct_size does not match the library");
+    if (cfg->abi_version != BH_GPU_ABI_VERSION)
+        return fail(ctx, BH_ERR_INVALID_ARG, "bh_render_config.abi_version does not match the library");
+    return BH_OK;
+}
+
+int ensure_table(bh_ctx* ctx) {
+    if (ctx->d_table) return BH_OK;
+    build_blackbody_table(ctx->h_table);
+    CK(cudaMalloc(&ctx->d_table, ctx->h_table.size() * sizeof(double)));
+    CK(cudaMemcpy(ctx->d_table, ctx->h_table.data(), ctx->h_table.size() * sizeof(double),
+                  cudaMemcpyHostToDevice));
+    return BH_OK;
+}
+
+int ensure_sky(bh_ctx* ctx, const bh_render_config& c) {
+    int rc = ensure_table(ctx);
+    if (rc != BH_OK) return rc;
+    const int count = c.stars_enabled ? c.star_count : 0;
+    if (ctx->sky_valid && ctx->sky_count == count && ctx->sky_seed == c.seed && ctx->sky_mode == c.sky_mode)
+        return BH_OK;
+    HostSky hs;
+    std::string err;
+    rc = build_sky(count, c.seed, c.sky_mode, ctx->h_table, hs, err);
+    if (rc != BH_OK) return fail(ctx, rc, err);
+    cudaFree(ctx->d_star_pos);
+    cudaFree(ctx->d_star_col);
+    cudaFree(ctx->d_bin_start);
+    ctx->d_star_pos = nullptr;
+    ctx->d_star_col = nullptr;
+    ctx->d_bin_start = nullptr;
+    ctx->sky_valid = false;
+    const size_t n = std::max<size_t>(hs.pos.size(), 1);
+    CK(cudaMalloc(&ctx->d_star_pos, n * sizeof(double4)));
+    CK(cudaMalloc(&ctx->d_star_col, n * sizeof(double4)));
+    CK(cudaMalloc(&ctx->d_bin_start, hs.bin_start.size() * sizeof(int32_t)));
+    if (!hs.pos.empty()) {
+        CK(cudaMemcpy(ctx->d_star_pos, hs.pos.data(), hs.pos.size() * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_star_col, hs.col.data(), hs.col.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy(ctx->d_bin_start, hs.bin_start.data(), hs.bin_start.size() * sizeof(int32_t),
+                  cudaMemcpyHostToDevice));
+    hs.pos.clear();
+    hs.col.clear();
+    ctx->sky_meta = std::move(hs);
+    ctx->sky_count = count;
+    ctx->sky_seed = c.seed;
+    ctx->sky_mode = c.sky_mode;
+    ctx->sky_valid = true;
+    return BH_OK;
+}
+
+SkyData sky_data(const bh_ctx* ctx) {
+    SkyData s;
+    std::memset(&s, 0, sizeof s);
+    s.star_pos = ctx->d_star_pos;
+    s.star_col = ctx->d_star_col;
+    s.bin_start = ctx->d_bin_start;
+    s.table = ctx->d_table;
+    s.mw_x = ctx->sky_meta.mw_x;
+    s.mw_z = ctx->sky_meta.mw_z;
+    s.mw_inv = ctx->sky_meta.mw_inv;
+    s.diffuse_L = ctx->sky_meta.diffuse_L;
+    s.n_stars = ctx->sky_count > 0 ? ctx->sky_count : 0;
+    return s;
+}
+
+void stats_add(bh_render_stats* s, const FrameStats& f) {
+    s->rays += (long long)f.rays;
+    s->steps += (long long)f.steps;
+    s->attempts += (long long)f.attempts;
+    s->captured += (long long)f.captured;
+    s->disc_hits += (long long)f.disc_hits;
+    s->sun_hits += (long long)f.sun_hits;
+    s->star_hits += (long long)f.star_hits;
+    s->escaped += (long long)f.escaped;
+    s->exhausted += (long long)f.exhausted;
+    double mn, mq;
+    std::memcpy(&mn, &f.max_norm_bits, sizeof mn);
+    std::memcpy(&mq, &f.max_q_bits, sizeof mq);
+    s->max_norm_error = std::max(s->max_norm_error, mn);
+    s->max_carter_drift = std::max(s->max_carter_drift, mq);
+    s->total_flux += f.total_flux;
+}
+
+// Enqueue the whole pipeline for `frames` on `stream`.  Pixels go to
+// `d_pixels` (frame-major, row-major), per-sample results to `d_rays` when
+// given (single frame only).
+int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_ray_result* d_rays,
+            cudaStream_t stream, bool timed) {
+    const int n = static_cast<int>(frames.size());
+    std::vector<long long> ray_end(n), pix_end(n);
+    long long rays = 0, pix = 0;
+    for (int i = 0; i < n; ++i) {
+        frames[i].ray_begin = rays;
+        frames[i].pixel_begin = pix;
+        rays += frames[i].n_rays;
+        pix += static_cast<long long>(frames[i].width) * frames[i].height;
+        ray_end[i] = rays;
+        pix_end[i] = pix;
+    }
+    int rc;
+    if ((rc = ensure(ctx, ctx->hits, static_cast<size_t>(rays) * sizeof(HitRecord))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->lum, static_cast<size_t>(pix) * sizeof(double))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->frames, n * sizeof(FrameParams))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->ray_end, n * sizeof(long long))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->pix_end, n * sizeof(long long))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->partials, static_cast<size_t>(n) * kReduceBlocks * sizeof(FrameStats))) != BH_OK)
+        return rc;
+    if ((rc = ensure(ctx, ctx->fstats, n * sizeof(FrameStats))) != BH_OK) return rc;
+
+    CK(cudaMemcpyAsync(ctx->frames.p, frames.data(), n * sizeof(FrameParams), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->ray_end.p, ray_end.data(), n * sizeof(long long), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->pix_end.p, pix_end.data(), n * sizeof(long long), cudaMemcpyHostToDevice, stream));
+    QueueState q;
+    std::memset(&q, 0, sizeof q);
+    q.budget = ctx->budget;
+    q.abort = ctx->abort_requested.load() ? 1 : 0;
+    CK(cudaMemcpyAsync(ctx->d_queue, &q, sizeof q, cudaMemcpyHostToDevice, stream));
+    ctx->h2d += static_cast<long long>(n * sizeof(FrameParams) + 2 * n * sizeof(long long) + sizeof q);
+
+    const bh_launch_params& lp = ctx->launch;
+    const int prec = frames[0].precision_tag;
+    int bps = lp.blocks_per_sm > 0 ? lp.blocks_per_sm : trace_blocks_per_sm(prec, lp.block_size);
+    if (bps < 1) bps = 1;
+    TraceLaunch tl;
+    tl.frames = static_cast<const FrameParams*>(ctx->frames.p);
+    tl.frame_ray_end = static_cast<const long long*>(ctx->ray_end.p);
+    tl.nframes = n;
+    tl.total_rays = rays;
+    tl.hits = static_cast<HitRecord*>(ctx->hits.p);
+    tl.queue = ctx->d_queue;
+    tl.precision = prec;
+    tl.block_size = lp.block_size;
+    tl.grid = ctx->sm_count * bps;
+    tl.rays_per_thread = lp.rays_per_thread;
+    tl.refill = lp.refill;
+    tl.budget = ctx->budget;
+    if (timed) CK(cudaEventRecord(ctx->ev[0], stream));
+    if (rays > 0) CK(launch_trace(tl, stream));
+    if (timed) CK(cudaEventRecord(ctx->ev[1], stream));
+
+    ShadeLaunch sl;
+    sl.frames = tl.frames;
+    sl.frame_pixel_end = static_cast<const long long*>(ctx->pix_end.p);
+    sl.nframes = n;
+    sl.total_pixels = pix;
+    sl.hits = tl.hits;
+    sl.sky = sky_data(ctx);
+    sl.pixels = d_pixels;
+    sl.rays = d_rays;
+    sl.pixel_lum = static_cast<double*>(ctx->lum.p);
+    sl.ray_class = nullptr;
+    CK(launch_shade(sl, stream));
+    if (timed) CK(cudaEventRecord(ctx->ev[2], stream));
+
+    ReduceLaunch rl;
+    rl.frames = tl.frames;
+    rl.nframes = n;
+    rl.hits = tl.hits;
+    rl.pixel_lum = sl.pixel_lum;
+    rl.partials = static_cast<FrameStats*>(ctx->partials.p);
+    rl.out = static_cast<FrameStats*>(ctx->fstats.p);
+    rl.blocks_per_frame = kReduceBlocks;
+    CK(launch_reduce(rl, stream));
+    return BH_OK;
+}
+
+// Read back the queue state and per-frame stats after the stream drained.
+int finish(bh_ctx* ctx, int n, bh_render_stats* per_frame, bh_render_stats* total, bool timed,
+           double seconds) {
+    QueueState q;
+    CK(cudaMemcpy(&q, ctx->d_queue, sizeof q, cudaMemcpyDeviceToHost));
+    std::vector<FrameStats> fs(n);
+    CK(cudaMemcpy(fs.data(), ctx->fstats.p, n * sizeof(FrameStats), cudaMemcpyDeviceToHost));
+    ctx->d2h += static_cast<long long>(sizeof q + n * sizeof(FrameStats));
+    float t_trace = 0.f, t_shade = 0.f;
+    if (timed) {
+        CK(cudaEventElapsedTime(&t_trace, ctx->ev[0], ctx->ev[1]));
+        CK(cudaEventElapsedTime(&t_shade, ctx->ev[1], ctx->ev[2]));
+    }
+    for (int i = 0; i < n; ++i) {
+        if (per_frame) {
+            stats_add(&per_frame[i], fs[i]);
+            per_frame[i].seconds = seconds;
+            per_frame[i].kernel_ms = t_trace;
+            per_frame[i].shade_ms = t_shade;
+            if (i == 0) {
+                per_frame[i].h2d_bytes += ctx->h2d;
+                per_frame[i].d2h_bytes += ctx->d2h;
+            }
+        }
+        if (total) stats_add(total, fs[i]);
+    }
+    if (total) {
+        total->h2d_bytes += ctx->h2d;
+        total->d2h_bytes += ctx->d2h;
+        total->seconds = seconds;
+        total->kernel_ms = t_trace;
+        total->shade_ms = t_shade;
+    }
+    if (q.abort == 1) return fail(ctx, BH_ERR_ABORTED, "launch aborted by bh_gpu_request_abort");
+    if (q.abort == 2) return fail(ctx, BH_ERR_BUDGET, "step budget of the launch exhausted");
+    return BH_OK;
+}
+
+int prepare_frames(bh_ctx* ctx, const bh_render_config* cfgs, int n, std::vector<FrameParams>& frames) {
+    ctx->h2d = 0;
+    ctx->d2h = 0;
+    frames.resize(n);
+    for (int i = 0; i < n; ++i) {
+        int rc = check_cfg_header(ctx, &cfgs[i]);
+        if (rc != BH_OK) return rc;
+        std::string err;
+        rc = make_frame(cfgs[i], frames[i], err);
+        if (rc != BH_OK) return fail(ctx, rc, n > 1 ? "frame " + std::to_string(i) + ": " + err : err);
+        frames[i].precision_tag = cfgs[i].precision;
+        if (i > 0) {
+            if (cfgs[i].precision != cfgs[0].precision)
+                return fail(ctx, BH_ERR_INVALID_ARG, "all frames of a batch must share the precision");
+            if ((cfgs[i].stars_enabled != 0) != (cfgs[0].stars_enabled != 0) ||
+                (cfgs[i].stars_enabled && (cfgs[i].star_count != cfgs[0].star_count ||
+                                           cfgs[i].seed != cfgs[0].seed ||
+                                           cfgs[i].sky_mode != cfgs[0].sky_mode)))
+                return fail(ctx, BH_ERR_INVALID_ARG, "all frames of a batch must share the star catalogue");
+        }
+    }
+    return ensure_sky(ctx, cfgs[0]);
+}
+
+}  // namespace
+
+extern "C" {
+
+int bh_gpu_abi_version(void) { return BH_GPU_ABI_VERSION; }
+
+void bh_render_config_default(bh_render_config* cfg) {
+    if (cfg) default_config(*cfg);
+}
+
+int bh_gpu_create(int device, bh_ctx** out) {
+    if (!out) return BH_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return BH_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) return BH_ERR_INVALID_ARG;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return BH_ERR_NO_DEVICE;
+    if (prop.major != 10) return BH_ERR_NO_DEVICE;   // built for sm_100a only
+    bh_ctx* ctx = new bh_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    auto bail = [&](cudaError_t e) {
+        bh_gpu_destroy(ctx);
+        return e == cudaErrorMemoryAllocation ? BH_ERR_OUT_OF_MEMORY : BH_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->abort_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    if ((e = cudaMalloc(&ctx->d_queue, sizeof(QueueState))) != cudaSuccess) return bail(e);
+    if ((e = cudaMemset(ctx->d_queue, 0, sizeof(QueueState))) != cudaSuccess) return bail(e);
+    if ((e = cudaHostAlloc(&ctx->h_one, sizeof(int32_t), cudaHostAllocDefault)) != cudaSuccess) return bail(e);
+    *ctx->h_one = 1;
+    for (auto& ev : ctx->ev)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
+    *out = ctx;
+    return BH_OK;
+}
+
+void bh_gpu_destroy(bh_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end,
+                      &ctx->pix_end, &ctx->partials, &ctx->fstats})
+        if (b->p) cudaFree(b->p);
+    cudaFree(ctx->d_table);
+    cudaFree(ctx->d_star_pos);
+    cudaFree(ctx->d_star_col);
+    cudaFree(ctx->d_bin_start);
+    cudaFree(ctx->d_queue);
+    if (ctx->h_one) cudaFreeHost(ctx->h_one);
+    for (auto& ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->abort_stream) cudaStreamDestroy(ctx->abort_stream);
+    delete ctx;
+}
+
+const char* bh_gpu_last_error(const bh_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int bh_gpu_render(bh_ctx* ctx, const bh_render_config* cfg, bh_xyz* out_pixels, bh_render_stats* stats) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!out_pixels) return fail(ctx, BH_ERR_INVALID_ARG, "out_pixels is NULL");
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    std::vector<FrameParams> frames;
+    int rc = prepare_frames(ctx, cfg, 1, frames);
+    if (rc != BH_OK) return rc;
+    const size_t npx = static_cast<size_t>(cfg->width) * cfg->height;
+    if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+    rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true);
+    if (rc != BH_OK) return rc;
+    CK(cudaMemcpyAsync(out_pixels, ctx->pixels.p, npx * sizeof(bh_xyz), cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->d2h += static_cast<long long>(npx * sizeof(bh_xyz));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    bh_render_stats local;
+    std::memset(&local, 0, sizeof local);
+    rc = finish(ctx, 1, nullptr, &local, true, secs);
+    if (stats) {
+        bh_render_stats s = local;
+        stats->rays += s.rays; stats->steps += s.steps; stats->captured += s.captured;
+        stats->disc_hits += s.disc_hits; stats->sun_hits += s.sun_hits; stats->star_hits += s.star_hits;
+        stats->jet_rays += s.jet_rays; stats->escaped += s.escaped; stats->exhausted += s.exhausted;
+        stats->total_flux += s.total_flux; stats->attempts += s.attempts;
+        stats->max_norm_error = std::max(stats->max_norm_error, s.max_norm_error);
+        stats->max_carter_drift = std::max(stats->max_carter_drift, s.max_carter_drift);
+        stats->seconds = s.seconds;
+        stats->kernel_ms = s.kernel_ms;
+        stats->shade_ms = s.shade_ms;
+        stats->h2d_bytes += s.h2d_bytes;
+        stats->d2h_bytes += s.d2h_bytes;
+    }
+    return rc;
+}
+
+int bh_gpu_render_device(bh_ctx* ctx, const bh_render_config* cfg, bh_xyz* d_pixels, bh_render_stats* stats,
+                         void* stream) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!d_pixels) return fail(ctx, BH_ERR_INVALID_ARG, "d_pixels is NULL");
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    std::vector<FrameParams> frames;
+    int rc = prepare_frames(ctx, cfg, 1, frames);
+    if (rc != BH_OK) return rc;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    rc = enqueue(ctx, frames, d_pixels, nullptr, s, stats != nullptr);
+    if (rc != BH_OK || !stats) return rc;
+    CK(cudaStreamSynchronize(s));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return finish(ctx, 1, stats, nullptr, true, secs);
+}
+
+int bh_gpu_trace_rays(bh_ctx* ctx, const bh_render_config* cfg, bh_ray_result* out, bh_render_stats* stats) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!out) return fail(ctx, BH_ERR_INVALID_ARG, "out is NULL");
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    std::vector<FrameParams> frames;
+    int rc = prepare_frames(ctx, cfg, 1, frames);
+    if (rc != BH_OK) return rc;
+    const size_t npx = static_cast<size_t>(cfg->width) * cfg->height;
+    const size_t nr = static_cast<size_t>(frames[0].n_rays);
+    if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->rays, nr * sizeof(bh_ray_result))) != BH_OK) return rc;
+    rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), static_cast<bh_ray_result*>(ctx->rays.p),
+                 ctx->stream, true);
+    if (rc != BH_OK) return rc;
+    CK(cudaMemcpyAsync(out, ctx->rays.p, nr * sizeof(bh_ray_result), cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->d2h += static_cast<long long>(nr * sizeof(bh_ray_result));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return finish(ctx, 1, stats, nullptr, true, secs);
+}
+
+int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz* const* outs,
+                        bh_render_stats* stats) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!cfgs || n <= 0 || !outs) return fail(ctx, BH_ERR_INVALID_ARG, "empty batch");
+    for (int i = 0; i < n; ++i)
+        if (!outs[i]) return fail(ctx, BH_ERR_INVALID_ARG, "outs[" + std::to_string(i) + "] is NULL");
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    std::vector<FrameParams> frames;
+    int rc = prepare_frames(ctx, cfgs, n, frames);
+    if (rc != BH_OK) return rc;
+    size_t npx = 0;
+    for (int i = 0; i < n; ++i) npx += static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
+    if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+    rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true);
+    if (rc != BH_OK) return rc;
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        const size_t m = static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
+        CK(cudaMemcpyAsync(outs[i], static_cast<bh_xyz*>(ctx->pixels.p) + off, m * sizeof(bh_xyz),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+        off += m;
+        ctx->d2h += static_cast<long long>(m * sizeof(bh_xyz));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return finish(ctx, n, stats, nullptr, true, secs);
+}
+
+int bh_gpu_set_launch(bh_ctx* ctx, const bh_launch_params* p) {
+    if (!ctx || !p) return BH_ERR_INVALID_ARG;
+    bh_launch_params n = ctx->launch;
+    if (p->block_size) {
+        if (p->block_size < 32 || p->block_size > 1024 || p->block_size % 32)
+            return fail(ctx, BH_ERR_INVALID_ARG, "block_size must be a multiple of 32 in [32, 1024]");
+        n.block_size = p->block_size;
+    }
+    if (p->rays_per_thread) {
+        if (p->rays_per_thread < 1 || p->rays_per_thread > 8)
+            return fail(ctx, BH_ERR_INVALID_ARG, "rays_per_thread must be in [1, 8]");
+        n.rays_per_thread = p->rays_per_thread;
+    }
+    if (p->refill) {
+        if (p->refill < 1 || p->refill > 32) return fail(ctx, BH_ERR_INVALID_ARG, "refill must be in [1, 32]");
+        n.refill = p->refill;
+    }
+    if (p->blocks_per_sm) {
+        if (p->blocks_per_sm < 0 || p->blocks_per_sm > 64)
+            return fail(ctx, BH_ERR_INVALID_ARG, "blocks_per_sm must be in [0, 64]");
+        n.blocks_per_sm = p->blocks_per_sm;
+    }
+    ctx->launch = n;
+    return BH_OK;
+}
+
+int bh_gpu_get_launch(const bh_ctx* ctx, bh_launch_params* p) {
+    if (!ctx || !p) return BH_ERR_INVALID_ARG;
+    *p = ctx->launch;
+    return BH_OK;
+}
+
+int bh_gpu_set_step_budget(bh_ctx* ctx, long long budget) {
+    if (!ctx || budget < 0) return BH_ERR_INVALID_ARG;
+    ctx->budget = static_cast<unsigned long long>(budget);
+    return BH_OK;
+}
+
+void bh_gpu_request_abort(bh_ctx* ctx) {
+    if (!ctx) return;
+    ctx->abort_requested.store(1);
+    cudaSetDevice(ctx->device);
+    // Lands in the queue state while a launch runs; the next launch starts
+    // with the flag set anyway.
+    cudaMemcpyAsync(&ctx->d_queue->abort, ctx->h_one, sizeof(int32_t), cudaMemcpyHostToDevice,
+                    ctx->abort_stream);
+}
+
+int bh_star_catalogue(int count, uint64_t seed, int sky_mode, double* out6) {
+    return star_catalogue(count, seed, sky_mode, out6);
+}
+
+int bh_blackbody_table(double* out) {
+    if (!out) return BH_ERR_INVALID_ARG;
+    std::vector<double> t;
+    build_blackbody_table(t);
+    std::memcpy(out, t.data(), t.size() * sizeof(double));
+    return BH_OK;
+}
+
+void bh_gpu_clear_abort(bh_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->abort_stream);
+    ctx->abort_requested.store(0);
+}
+
+}  // extern "C"

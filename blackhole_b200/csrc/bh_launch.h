@@ -1,0 +1,63 @@
+// bh_launch.h - Host-side launch wrappers of the device kernels (bh_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bh_frame.h"
+
+struct bh_xyz;
+struct bh_ray_result;
+
+namespace bhg {
+
+struct TraceLaunch {
+    const FrameParams* frames;       // device array
+    const long long* frame_ray_end;  // device array: cumulative ray counts (exclusive end)
+    int nframes;
+    long long total_rays;
+    HitRecord* hits;                 // device, total_rays entries
+    QueueState* queue;               // device
+    int precision;                   // BH_PRECISION_*
+    int block_size;
+    int grid;                        // blocks
+    int rays_per_thread;
+    int refill;
+    unsigned long long budget;       // step-attempt budget of the launch, 0 = none
+};
+
+// Persistent trace kernel over all rays of all frames.
+cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream);
+
+// Blocks per SM that fit for a precision and block size (occupancy query).
+int trace_blocks_per_sm(int precision, int block_size);
+// Registers per thread of the trace kernel of a precision (for reports).
+int trace_registers(int precision);
+
+struct ShadeLaunch {
+    const FrameParams* frames;
+    const long long* frame_pixel_end;   // cumulative pixel counts
+    int nframes;
+    long long total_pixels;
+    const HitRecord* hits;
+    SkyData sky;
+    bh_xyz* pixels;                  // device, total_pixels entries (frame-major, row-major)
+    bh_ray_result* rays;             // optional device per-sample results (single frame)
+    double* pixel_lum;               // device, total_pixels luminance for the flux sum
+    unsigned char* ray_class;        // device, per-ray class after shading
+};
+
+cudaError_t launch_shade(const ShadeLaunch& L, cudaStream_t stream);
+
+struct ReduceLaunch {
+    const FrameParams* frames;
+    int nframes;
+    const HitRecord* hits;
+    const double* pixel_lum;
+    FrameStats* partials;            // nframes * blocks_per_frame
+    FrameStats* out;                 // nframes
+    int blocks_per_frame;
+};
+
+cudaError_t launch_reduce(const ReduceLaunch& L, cudaStream_t stream);
+
+}  // namespace bhg

@@ -1,0 +1,117 @@
+"""Named render workloads.
+
+Each function returns a ``RenderConfig`` (or a list of them) for one of the
+measured scenes.  Common to all of them: observer at r = 1000 M (unless
+stated), field of view covering +-25 M at the hole (fov = 2 atan(25/1000)),
+one sample per pixel, escape radius 1.1 r_obs, horizon stop at
+r_+ (1 + 1e-6), and a seeded 250,000-star sky that is isotropic, with
+magnitudes from log N(<m) = 0.45 m up to m = 6.5, B-V uniform in
+[-0.3, 1.8] and a uniform 21.5 mag/arcsec^2 diffuse background.
+"""
+from __future__ import annotations
+
+import math
+import random
+
+from . import abi
+from .config import M_SUN, Camera, RenderConfig
+
+R_OBS = 1000.0
+
+
+def _fov(half_width_m: float, r_obs: float = R_OBS) -> float:
+    return 2.0 * math.atan(half_width_m / r_obs)
+
+
+def _base(**kw) -> RenderConfig:
+    cfg = RenderConfig(
+        sqrt_spp=1,
+        rtol=1e-8,
+        atol=1e-10,
+        r_escape=1.1 * R_OBS,
+        star_count=250000,
+        seed=20240921,
+        sky_mode=abi.SKY_UNIFORM,
+        stop_mode=abi.STOP_RELATIVE,
+        stop_epsilon=1e-6,
+        quiet=True,
+    )
+    for k, v in kw.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def kerr_fp64_256() -> RenderConfig:
+    """Plain FP64 render, 256x256: a = 0.9, inclination 60 deg,
+    M = 4.3e6 M_sun, disc r_isco..30 M at 0.1 Eddington."""
+    return _base(
+        M_kg=4.3e6 * M_SUN, spin=0.9,
+        cam=Camera(r=R_OBS, theta=math.radians(60.0), phi=0.0, fov=_fov(25.0)),
+        width=256, height=256, disc_r_out=30.0, eddington=0.1,
+        precision=abi.PRECISION_FP64,
+    )
+
+
+def edge_on_1024(precision: int = abi.PRECISION_MIXED) -> RenderConfig:
+    """1024x1024 near edge-on frame: a = 0.998, inclination 85 deg,
+    M = 10 M_sun, disc r_isco..50 M at 0.3 Eddington."""
+    return _base(
+        M_kg=10.0 * M_SUN, spin=0.998,
+        cam=Camera(r=R_OBS, theta=math.radians(85.0), phi=0.0, fov=_fov(25.0)),
+        width=1024, height=1024, disc_r_out=50.0, eddington=0.3,
+        precision=precision,
+    )
+
+
+def batch_64_frames(seed: int = 64, precision: int = abi.PRECISION_MIXED) -> list:
+    """64 frames of uneven size in a seeded shuffle: spins {0, 0.5, 0.9, 0.998}
+    x inclinations {15, 45, 70, 85} deg x resolutions {256, 512, 1024, 2048}^2
+    (every combination once), observer radius uniform in [500, 2000] M, disc
+    r_isco..30 M at 0.1 Eddington, M = 4.3e6 M_sun.  The field of view keeps
+    +-25 M at each observer radius."""
+    rng = random.Random(seed)
+    combos = [(a, i, n) for a in (0.0, 0.5, 0.9, 0.998) for i in (15.0, 45.0, 70.0, 85.0)
+              for n in (256, 512, 1024, 2048)]
+    rng.shuffle(combos)
+    frames = []
+    for a, inc, n in combos:
+        r_obs = rng.uniform(500.0, 2000.0)
+        frames.append(_base(
+            M_kg=4.3e6 * M_SUN, spin=a,
+            cam=Camera(r=r_obs, theta=math.radians(inc), phi=0.0, fov=_fov(25.0, r_obs)),
+            width=n, height=n, disc_r_out=30.0, eddington=0.1,
+            r_escape=1.1 * r_obs, precision=precision,
+        ))
+    return frames
+
+
+def adjoint_512(target: bool = False) -> RenderConfig:
+    """512x512 luminance frame for the gradient check: a = 0.7, inclination
+    50 deg, 0.2 Eddington, r_out = 25 M (target: a = 0.75, 53 deg, 0.22,
+    27 M), M = 4.3e6 M_sun."""
+    if target:
+        a, inc, edd, r_out = 0.75, 53.0, 0.22, 27.0
+    else:
+        a, inc, edd, r_out = 0.7, 50.0, 0.2, 25.0
+    return _base(
+        M_kg=4.3e6 * M_SUN, spin=a,
+        cam=Camera(r=R_OBS, theta=math.radians(inc), phi=0.0, fov=_fov(25.0)),
+        width=512, height=512, disc_r_out=r_out, eddington=edd,
+        precision=abi.PRECISION_FP64,
+    )
+
+
+def photon_ring_4096(precision: int = abi.PRECISION_MIXED, size: int = 4096) -> RenderConfig:
+    """Narrow +-8 M frame at a = 0.998, inclination 75 deg, M = 6.5e9 M_sun,
+    disc r_isco..100 M at 0.5 Eddington, aimed (yaw) at the prograde edge of
+    the critical curve so many rays orbit before escaping or falling in."""
+    cfg = _base(
+        M_kg=6.5e9 * M_SUN, spin=0.998,
+        cam=Camera(r=R_OBS, theta=math.radians(75.0), phi=0.0, fov=_fov(8.0)),
+        width=size, height=size, disc_r_out=100.0, eddington=0.5,
+        precision=precision,
+    )
+    # The prograde photon orbit of a = 0.998 sits at about b = 2.2 M on the
+    # approaching side; centre the frame there.
+    cfg.cam.yaw = math.atan(-2.2 / R_OBS)
+    return cfg

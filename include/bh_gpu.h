@@ -1,0 +1,271 @@
+/*
+ * bh_gpu.h - C-ABI of the B200 geodesic render library (libbh_gpu.so).
+ *
+ * This is the drop-in boundary for the reference renderer's per-pixel loop:
+ *
+ *     img::Image bh::render(const RenderConfig& cfg, RenderStats& stats);   (render.h:72)
+ *
+ * The POD structs below mirror bh::RenderConfig (render.h:15-53), bh::Camera
+ * (scene.h:343-351), bh::RenderStats (render.h:55-69) and the img::Image pixel
+ * layout (image.h:18-27: row-major vector<spec::XYZ>, spec::XYZ = 3 doubles,
+ * spectrum.h:23-25).  No C++ or CUDA types cross this boundary: plain pointers,
+ * sizes and status codes only.
+ *
+ * Conventions
+ *  - Every entry point that can fail returns 0 (BH_OK) or a negative bh_status.
+ *    The message of the last failure on a context is bh_gpu_last_error().
+ *  - Host buffers are owned by the caller.  A context owns its device memory
+ *    (ray buffers, star catalogue, spectrum table) and reuses it across calls.
+ *  - One context per host thread; a context drives one GPU.  Calls on one
+ *    context are serialised by the caller (like a CUDA stream).
+ *  - Stats follow bh::render: counters and the two drift maxima are ADDED
+ *    into *stats (render.cpp:481-494); `seconds` is overwritten (render.cpp:495).
+ *  - There is no CPU fallback: without a usable GPU, bh_gpu_create fails with
+ *    BH_ERR_NO_DEVICE.
+ */
+#ifndef BH_GPU_H
+#define BH_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BH_GPU_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+    BH_OK = 0,
+    BH_ERR_INVALID_ARG = -1,   /* a config field or pointer is out of range        */
+    BH_ERR_CUDA = -2,          /* a CUDA runtime call failed                       */
+    BH_ERR_BUDGET = -3,        /* the per-launch step budget ran out               */
+    BH_ERR_ABORTED = -4,       /* bh_gpu_request_abort() stopped the launch        */
+    BH_ERR_NO_DEVICE = -5,     /* no CUDA device, or not an sm_100 part            */
+    BH_ERR_UNSUPPORTED = -6,   /* a feature of the config that is not built        */
+    BH_ERR_OUT_OF_MEMORY = -7  /* device allocation failed                         */
+};
+
+/* Termination class of a ray; same order as Hit::What (render.cpp:37). */
+enum {
+    BH_HIT_HORIZON = 0,
+    BH_HIT_DISC = 1,
+    BH_HIT_SUN = 2,
+    BH_HIT_STAR = 3,      /* neutron-star surface */
+    BH_HIT_SKY = 4,
+    BH_HIT_EXHAUSTED = 5
+};
+
+/* Arithmetic of the integrator (extension; the reference is FP64 only). */
+enum {
+    BH_PRECISION_FP64 = 0,   /* every operation in IEEE binary64                   */
+    BH_PRECISION_MIXED = 1   /* binary32 state and stages; binary64 for Delta and
+                                Sigma, the error norm, accept/reject, h, root
+                                refinement and the invariant diagnostics           */
+};
+
+/* Background sky (extension). */
+enum {
+    BH_SKY_GALACTIC = 0,     /* the reference catalogue: 45% galactic band, m <= 12,
+                                normal B-V, plus the band-modulated Milky Way
+                                (scene.h:62-107, 202-223)                          */
+    BH_SKY_UNIFORM = 1       /* isotropic stars, m <= 6.5, B-V uniform in
+                                [-0.3, 1.8], plus a uniform 21.5 mag/arcsec^2
+                                background                                          */
+};
+
+/* Horizon stop radius (extension). */
+enum {
+    BH_STOP_REFERENCE = 0,   /* r_+ + 1e-4 + 1e-3 (r_+ - r_-)    (render.cpp:73)    */
+    BH_STOP_RELATIVE = 1     /* r_+ (1 + stop_epsilon)                               */
+};
+
+typedef struct bh_xyz {      /* spec::XYZ (spectrum.h:23-25), W m^-2 sr^-1 */
+    double x, y, z;
+} bh_xyz;
+
+typedef struct bh_camera {   /* bh::Camera (scene.h:343-351) */
+    double r, theta, phi;    /* Boyer-Lindquist position                    */
+    double fov;              /* horizontal field of view, radians           */
+    double yaw, pitch, roll;
+} bh_camera;
+
+typedef struct bh_sun {      /* bh::SunBody (scene.h:232-236) */
+    double centre[3];        /* pseudo-Cartesian, gravitational radii */
+    double radius;
+    double T_eff;
+} bh_sun;
+
+typedef struct bh_hotspot {  /* bh::HotSpot (scene.h:306-313) */
+    int32_t enabled;
+    int32_t sense;
+    double r, phi0, sigma, contrast, omega;
+} bh_hotspot;
+
+typedef struct bh_neutron_star {  /* bh::NeutronStar (neutronstar.h:43-70) */
+    int32_t enabled;
+    int32_t caps;
+    double M_kg, R_m, R;     /* R in gravitational radii */
+    double T_eff;
+    double spin_hz, Omega;
+    double cap_tilt, cap_radius, cap_T, cap_phase0;
+    int32_t two_caps;
+    int32_t reserved;
+} bh_neutron_star;
+
+/* bh::RenderConfig (render.h:15-53) plus the GPU extensions at the end. */
+typedef struct bh_render_config {
+    uint32_t struct_size;    /* sizeof(bh_render_config) as the caller compiled it */
+    uint32_t abi_version;    /* BH_GPU_ABI_VERSION                                 */
+
+    double M_kg;
+    double spin;
+    bh_camera cam;
+    int32_t width, height;
+    int32_t sqrt_spp;
+
+    int32_t disc_enabled;
+    double disc_r_out;
+    double eddington;
+    int32_t disc_sense;
+    int32_t stars_enabled;
+    int32_t star_count;
+    int32_t sun_enabled;
+    uint64_t seed;
+    bh_sun sun;
+    bh_hotspot hotspot;
+    bh_neutron_star star;
+    int32_t jet_enabled;     /* jets are not built: must be 0 */
+    int32_t reserved0;
+
+    double observer_time;
+
+    double rtol, atol;
+    double r_escape;
+    int32_t max_steps;
+
+    int32_t threads;         /* accepted and ignored (the GPU launch replaces the pool) */
+    int32_t quiet;           /* accepted and ignored */
+
+    /* ---- extensions ------------------------------------------------------ */
+    int32_t precision;       /* BH_PRECISION_*                                   */
+    int32_t sky_mode;        /* BH_SKY_*                                         */
+    int32_t stop_mode;       /* BH_STOP_*                                        */
+    int32_t milky_way;       /* diffuse background on (1) / off (0)              */
+    double stop_epsilon;     /* BH_STOP_RELATIVE only                            */
+    double mixed_rtol;       /* tolerances of the MIXED path; 0 = max(rtol, 1e-6) */
+    double mixed_atol;       /*                               0 = max(atol, 1e-8) */
+} bh_render_config;
+
+/* bh::RenderStats (render.h:55-69) plus extensions. */
+typedef struct bh_render_stats {
+    long long rays;
+    long long steps;         /* accepted integration steps */
+    long long captured;
+    long long disc_hits;
+    long long sun_hits;
+    long long star_hits;
+    long long jet_rays;
+    long long escaped;
+    long long exhausted;
+    double max_norm_error;   /* worst |g^ab p_a p_b| / sum |terms| along any ray */
+    double max_carter_drift; /* worst |Q - Q0| / (|Q0| + 1e-12)                  */
+    double seconds;
+    double total_flux;       /* sum of pixel luminance Y                         */
+    /* ---- extensions ---- */
+    long long attempts;      /* step attempts, accepted + rejected               */
+    double kernel_ms;        /* device time of the trace kernel                  */
+    double shade_ms;         /* device time of the shade kernel                  */
+    long long h2d_bytes;     /* host->device bytes the call copied               */
+    long long d2h_bytes;     /* device->host bytes the call copied               */
+} bh_render_stats;
+
+/* Per-sample result, for parity checks (the fields trace() and shade() see). */
+typedef struct bh_ray_result {
+    int32_t what;            /* BH_HIT_*                                         */
+    int32_t steps;           /* accepted steps of this ray                       */
+    double y[8];             /* final state (t, r, th, phi, p_t, p_r, p_th, p_phi) */
+    double g;                /* redshift factor of a disc hit, else 0           */
+    double dir[3];           /* unit sky direction of an escaped ray, else 0    */
+    bh_xyz xyz;              /* radiance of this sample                          */
+} bh_ray_result;
+
+/* Launch shape of the persistent trace kernel (the autotuner's search space). */
+typedef struct bh_launch_params {
+    int32_t block_size;      /* threads per block, multiple of 32, 64..512       */
+    int32_t rays_per_thread; /* rays a lane takes per queue visit, 1..4          */
+    int32_t refill;          /* lanes that must be idle before a warp refills   */
+    int32_t blocks_per_sm;   /* 0 = as many as fit                              */
+} bh_launch_params;
+
+typedef struct bh_ctx bh_ctx;
+
+int  bh_gpu_abi_version(void);
+
+/* The reference's defaults (render.h:15-53, scene.h:343-351) plus
+   BH_PRECISION_FP64, BH_SKY_GALACTIC, BH_STOP_REFERENCE, milky_way = 1. */
+void bh_render_config_default(bh_render_config* cfg);
+
+int  bh_gpu_create(int device, bh_ctx** out);
+void bh_gpu_destroy(bh_ctx* ctx);
+const char* bh_gpu_last_error(const bh_ctx* ctx);
+
+/* Replaces bh::render (render.cpp:396-497): trace and shade every sample of
+   the frame, write W*H pixels (row-major, averaged over sqrt_spp^2 samples)
+   into the caller's host buffer and add the frame's counters into *stats
+   (stats may be NULL). */
+int  bh_gpu_render(bh_ctx* ctx, const bh_render_config* cfg,
+                   bh_xyz* out_pixels, bh_render_stats* stats);
+
+/* The same frame, written into a device buffer of W*H bh_xyz on `stream`
+   (a cudaStream_t, or NULL for the context's stream).  Returns once the work
+   is enqueued when stats == NULL; with stats it synchronises. */
+int  bh_gpu_render_device(bh_ctx* ctx, const bh_render_config* cfg,
+                          bh_xyz* d_pixels, bh_render_stats* stats, void* stream);
+
+/* Per-sample results of a whole frame: W*H*sqrt_spp^2 entries, ordered by
+   pixel (row-major) and then by sample (sy, sx) as in render.cpp:439-456. */
+int  bh_gpu_trace_rays(bh_ctx* ctx, const bh_render_config* cfg,
+                       bh_ray_result* out, bh_render_stats* stats);
+
+/* Many frames of any size in one persistent launch (replaces the serial frame
+   loop of main.cpp:952-989).  outs[i] receives frame i's pixels; stats[i]
+   (optional array) receives frame i's counters.  All frames must share the
+   precision, sky and star settings of cfgs[0]. */
+int  bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n,
+                         bh_xyz* const* outs, bh_render_stats* stats);
+
+/* Launch shape used by the next calls; zero fields keep the current value. */
+int  bh_gpu_set_launch(bh_ctx* ctx, const bh_launch_params* p);
+int  bh_gpu_get_launch(const bh_ctx* ctx, bh_launch_params* p);
+
+/* Step budget of one launch (total step attempts over all rays; 0 = none).
+   A launch that exceeds it stops taking rays and returns BH_ERR_BUDGET. */
+int  bh_gpu_set_step_budget(bh_ctx* ctx, long long budget);
+
+/* Ask the next or running launch on this context to stop taking rays; it then
+   returns BH_ERR_ABORTED.  Safe to call from another host thread. */
+void bh_gpu_request_abort(bh_ctx* ctx);
+void bh_gpu_clear_abort(bh_ctx* ctx);
+
+/* Measured FMA throughput of `device` in TFLOP/s (2 FLOP per FMA) for
+   BH_PRECISION_FP64 (binary64) or BH_PRECISION_MIXED (binary32): the ALU
+   roofline of the trace kernel.  Extension; no counterpart in the reference. */
+int  bh_gpu_fma_peak(int device, int precision, double* tflops);
+
+/* The star catalogue the render path uploads for (count, seed, sky_mode): six
+   doubles per star (x, y, z, magnitude, temperature K, irradiance W m^-2) in
+   generation order, as StarField builds it (scene.h:62-104).  Host-side; needs
+   no GPU.  Replaces nothing: exposes the catalogue for inspection. */
+int  bh_star_catalogue(int count, uint64_t seed, int sky_mode, double* out6);
+
+/* ln X, ln Y, ln Z of the 4096-entry blackbody table the GPU reads
+   (spectrum.cpp:94-121), 3*4096 doubles.  Host-side; needs no GPU. */
+int  bh_blackbody_table(double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BH_GPU_H */

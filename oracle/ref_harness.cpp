@@ -1,0 +1,379 @@
+// ref_harness.cpp - C entry points onto the reference renderer itself.
+//
+// TEST INFRASTRUCTURE.  This translation unit includes the reference's
+// render.cpp (and through it kerr.h, geodesic.h, disc.h, scene.h) and is
+// linked with the reference's spectrum.cpp, all compiled unmodified from the
+// reference tree into oracle/_ref/libbh_ref.so by oracle/Makefile.  It gives
+// the tests and the CPU baseline access to:
+//   - ref_render:        the reference's own bh::render (render.cpp:396-497);
+//   - ref_render_rows:   the reference's trace() + shade() over a set of rows,
+//                        in a row-atomic std::thread pool like render() uses
+//                        (render.cpp:420-477), for bounded timing samples;
+//   - ref_trace_rays:    per-sample trace()/shade() results of a pixel window;
+//   - ref_* functions:   the known-answer quantities of validate.cpp.
+// Nothing here is shipped or called by the GPU library.
+
+// Standard headers first, so that the access override below touches only the
+// reference's own classes (StarField keeps its catalogue private).
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#define private public
+#include "render.cpp"
+#undef private
+
+#include "../include/bh_gpu.h"
+
+namespace {
+
+bh::RenderConfig to_ref(const bh_render_config& c) {
+    bh::RenderConfig r;
+    r.M_kg = c.M_kg;
+    r.spin = c.spin;
+    r.cam.r = c.cam.r;
+    r.cam.theta = c.cam.theta;
+    r.cam.phi = c.cam.phi;
+    r.cam.fov = c.cam.fov;
+    r.cam.yaw = c.cam.yaw;
+    r.cam.pitch = c.cam.pitch;
+    r.cam.roll = c.cam.roll;
+    r.width = c.width;
+    r.height = c.height;
+    r.sqrt_spp = c.sqrt_spp;
+    r.disc_enabled = c.disc_enabled != 0;
+    r.disc_r_out = c.disc_r_out;
+    r.eddington = c.eddington;
+    r.disc_sense = c.disc_sense;
+    r.stars_enabled = c.stars_enabled != 0;
+    r.star_count = c.star_count;
+    r.seed = c.seed;
+    r.sun_enabled = c.sun_enabled != 0;
+    for (int i = 0; i < 3; ++i) r.sun.centre[i] = c.sun.centre[i];
+    r.sun.radius = c.sun.radius;
+    r.sun.T_eff = c.sun.T_eff;
+    r.hotspot.enabled = c.hotspot.enabled != 0;
+    r.hotspot.r = c.hotspot.r;
+    r.hotspot.phi0 = c.hotspot.phi0;
+    r.hotspot.sigma = c.hotspot.sigma;
+    r.hotspot.contrast = c.hotspot.contrast;
+    r.hotspot.omega = c.hotspot.omega;
+    r.hotspot.sense = c.hotspot.sense;
+    r.star.enabled = c.star.enabled != 0;
+    r.star.caps = c.star.caps != 0;
+    r.star.M_kg = c.star.M_kg;
+    r.star.R_m = c.star.R_m;
+    r.star.R = c.star.R;
+    r.star.T_eff = c.star.T_eff;
+    r.star.spin_hz = c.star.spin_hz;
+    r.star.Omega = c.star.Omega;
+    r.star.cap_tilt = c.star.cap_tilt;
+    r.star.cap_radius = c.star.cap_radius;
+    r.star.cap_T = c.star.cap_T;
+    r.star.cap_phase0 = c.star.cap_phase0;
+    r.star.two_caps = c.star.two_caps != 0;
+    r.jet.enabled = false;
+    r.observer_time = c.observer_time;
+    r.rtol = c.rtol;
+    r.atol = c.atol;
+    r.r_escape = c.r_escape;
+    r.max_steps = c.max_steps;
+    r.threads = c.threads;
+    r.quiet = true;
+    return r;
+}
+
+int check_cfg(const bh_render_config* c) {
+    if (!c || c->width <= 0 || c->height <= 0) return BH_ERR_INVALID_ARG;
+    // The reference has one sky, one stop rule and no jet hook here.
+    if (c->jet_enabled || c->sky_mode != BH_SKY_GALACTIC || c->stop_mode != BH_STOP_REFERENCE)
+        return BH_ERR_UNSUPPORTED;
+    return BH_OK;
+}
+
+void stats_out(const bh::RenderStats& s, bh_render_stats* o) {
+    if (!o) return;
+    o->rays += s.rays;
+    o->steps += s.steps;
+    o->captured += s.captured;
+    o->disc_hits += s.disc_hits;
+    o->sun_hits += s.sun_hits;
+    o->star_hits += s.star_hits;
+    o->jet_rays += s.jet_rays;
+    o->escaped += s.escaped;
+    o->exhausted += s.exhausted;
+    o->total_flux += s.total_flux;
+    o->max_norm_error = std::max(o->max_norm_error, s.max_norm_error);
+    o->max_carter_drift = std::max(o->max_carter_drift, s.max_carter_drift);
+    o->seconds = s.seconds;
+}
+
+// Everything render() builds before its pixel loop (render.cpp:396-418).
+struct Scene {
+    bh::RenderConfig cfg;
+    std::unique_ptr<bh::NovikovThorneDisc> disc;
+    std::unique_ptr<bh::StarField> stars;
+    bh::Tetrad tet;
+    double aspect, psf_sigma;
+    spec::XYZ jet_colour;
+    explicit Scene(const bh_render_config& c, bool milky_way) : cfg(to_ref(c)) {
+        if (cfg.disc_enabled)
+            disc = std::make_unique<bh::NovikovThorneDisc>(cfg.M_kg, cfg.spin, cfg.disc_r_out,
+                                                           cfg.eddington, cfg.disc_sense);
+        if (cfg.stars_enabled)
+            stars = std::make_unique<bh::StarField>(cfg.star_count, cfg.seed, milky_way);
+        const bh::Geom gcam = bh::geom_at(cfg.spin, cfg.cam.r, cfg.cam.theta);
+        tet = bh::zamo_tetrad(gcam);
+        aspect = static_cast<double>(cfg.width) / cfg.height;
+        psf_sigma = 0.55 * (cfg.cam.fov / cfg.width);
+        jet_colour = spec::XYZ{};
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int ref_render(const bh_render_config* c, bh_xyz* out, bh_render_stats* st) {
+    const int rc = check_cfg(c);
+    if (rc != BH_OK) return rc;
+    if (!c->milky_way && c->stars_enabled) return BH_ERR_UNSUPPORTED;
+    const bh::RenderConfig cfg = to_ref(*c);
+    bh::RenderStats s;
+    const img::Image im = bh::render(cfg, s);
+    if (out) std::memcpy(out, im.pixels.data(), im.pixels.size() * sizeof(spec::XYZ));
+    stats_out(s, st);
+    return BH_OK;
+}
+
+// The pixel loop of render.cpp:428-463 restricted to the listed rows, on
+// `threads` workers pulling rows from an atomic counter.  Pixels go to
+// out[k * width + x] for the k-th listed row.  Scene setup (disc, star
+// catalogue, spectrum table) is done before the clock starts and reported in
+// st->seconds separately from tracing: *setup_seconds gets the setup time.
+int ref_render_rows(const bh_render_config* c, const int* rows, int nrows, int threads,
+                    bh_xyz* out, bh_render_stats* st, double* setup_seconds) {
+    const int rc = check_cfg(c);
+    if (rc != BH_OK) return rc;
+    if (nrows < 0 || (nrows > 0 && !rows)) return BH_ERR_INVALID_ARG;
+    for (int k = 0; k < nrows; ++k)
+        if (rows[k] < 0 || rows[k] >= c->height) return BH_ERR_INVALID_ARG;
+    const auto t_setup = std::chrono::steady_clock::now();
+    Scene sc(*c, c->milky_way != 0);
+    (void)spec::blackbody_xyz(5000.0);  // build the magic-static table outside the clock
+    const auto t_start = std::chrono::steady_clock::now();
+    if (setup_seconds)
+        *setup_seconds = std::chrono::duration<double>(t_start - t_setup).count();
+
+    int nthreads = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
+    if (nthreads <= 0) nthreads = 1;
+    std::atomic<int> next{0};
+    std::vector<bh::RenderStats> per_thread(nthreads);
+    const bh::RenderConfig& cfg = sc.cfg;
+    auto worker = [&](int tid) {
+        bh::RenderStats& local = per_thread[tid];
+        const int S = std::max(1, cfg.sqrt_spp);
+        const double inv_S = 1.0 / S;
+        for (;;) {
+            const int k = next.fetch_add(1);
+            if (k >= nrows) break;
+            const int y = rows[k];
+            for (int x = 0; x < cfg.width; ++x) {
+                bh::Rng rng(cfg.seed ^ (static_cast<uint64_t>(y) << 32) ^
+                            (static_cast<uint64_t>(x) * 0x9E3779B97F4A7C15ull));
+                spec::XYZ acc{};
+                for (int sy = 0; sy < S; ++sy)
+                    for (int sx = 0; sx < S; ++sx) {
+                        const double jx = (sx + rng.uniform()) * inv_S;
+                        const double jy = (sy + rng.uniform()) * inv_S;
+                        const double u = (2.0 * (x + jx) / cfg.width - 1.0);
+                        const double v = (1.0 - 2.0 * (y + jy) / cfg.height);
+                        double dir[3];
+                        cfg.cam.ray_direction(u, v, sc.aspect, dir);
+                        ++local.rays;
+                        const bh::Hit hit = bh::trace(cfg, sc.disc.get(), dir, sc.tet, local);
+                        const spec::XYZ col = bh::shade(cfg, sc.disc.get(), sc.stars.get(), hit,
+                                                        sc.psf_sigma, sc.jet_colour, local);
+                        acc.x += col.x; acc.y += col.y; acc.z += col.z;
+                    }
+                const double w = 1.0 / (S * S);
+                if (out) out[static_cast<size_t>(k) * cfg.width + x] = {acc.x * w, acc.y * w, acc.z * w};
+                local.total_flux += acc.y * w;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t) pool.emplace_back(worker, t);
+    for (auto& th : pool) th.join();
+    bh::RenderStats total;
+    for (const auto& s : per_thread) {
+        total.rays += s.rays; total.steps += s.steps; total.captured += s.captured;
+        total.disc_hits += s.disc_hits; total.sun_hits += s.sun_hits; total.star_hits += s.star_hits;
+        total.jet_rays += s.jet_rays; total.escaped += s.escaped; total.exhausted += s.exhausted;
+        total.total_flux += s.total_flux;
+        total.max_norm_error = std::max(total.max_norm_error, s.max_norm_error);
+        total.max_carter_drift = std::max(total.max_carter_drift, s.max_carter_drift);
+    }
+    total.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    stats_out(total, st);
+    return BH_OK;
+}
+
+// Per-sample trace()/shade() results of a pixel window, single-threaded.
+int ref_trace_rays(const bh_render_config* c, int x0, int y0, int w, int h, bh_ray_result* out,
+                   bh_render_stats* st) {
+    const int rc = check_cfg(c);
+    if (rc != BH_OK) return rc;
+    if (x0 < 0 || y0 < 0 || w < 0 || h < 0 || x0 + w > c->width || y0 + h > c->height)
+        return BH_ERR_INVALID_ARG;
+    Scene sc(*c, c->milky_way != 0);
+    const bh::RenderConfig& cfg = sc.cfg;
+    bh::RenderStats local;
+    const int S = std::max(1, cfg.sqrt_spp);
+    const double inv_S = 1.0 / S;
+    size_t idx = 0;
+    for (int y = y0; y < y0 + h; ++y)
+        for (int x = x0; x < x0 + w; ++x) {
+            bh::Rng rng(cfg.seed ^ (static_cast<uint64_t>(y) << 32) ^
+                        (static_cast<uint64_t>(x) * 0x9E3779B97F4A7C15ull));
+            spec::XYZ acc{};
+            for (int sy = 0; sy < S; ++sy)
+                for (int sx = 0; sx < S; ++sx) {
+                    const double jx = (sx + rng.uniform()) * inv_S;
+                    const double jy = (sy + rng.uniform()) * inv_S;
+                    const double u = (2.0 * (x + jx) / cfg.width - 1.0);
+                    const double v = (1.0 - 2.0 * (y + jy) / cfg.height);
+                    double dir[3];
+                    cfg.cam.ray_direction(u, v, sc.aspect, dir);
+                    ++local.rays;
+                    const long long steps0 = local.steps;
+                    const bh::Hit hit = bh::trace(cfg, sc.disc.get(), dir, sc.tet, local);
+                    const spec::XYZ col = bh::shade(cfg, sc.disc.get(), sc.stars.get(), hit,
+                                                    sc.psf_sigma, sc.jet_colour, local);
+                    acc.x += col.x; acc.y += col.y; acc.z += col.z;
+                    bh_ray_result& o = out[idx++];
+                    std::memset(&o, 0, sizeof o);
+                    o.what = static_cast<int32_t>(hit.what);
+                    o.steps = static_cast<int32_t>(local.steps - steps0);
+                    for (int i = 0; i < 8; ++i) o.y[i] = hit.y[i];
+                    o.xyz.x = col.x; o.xyz.y = col.y; o.xyz.z = col.z;
+                    // The fields shade_hit computes on the way (render.cpp:275-325).
+                    if (hit.what == bh::Hit::What::Disc && sc.disc) {
+                        const double r = hit.y[bh::Y_R];
+                        if (sc.disc->temperature(r) > 0.0) {
+                            const double g = bh::redshift_factor(hit.y, sc.disc->four_velocity(r));
+                            o.g = (g > 0.0) ? g : 0.0;
+                        }
+                    } else if (hit.what == bh::Hit::What::Sky) {
+                        const bh::State d = bh::geodesic_rhs(cfg.spin, hit.y);
+                        double v3[3];
+                        bh::cartesian_velocity(cfg.spin, hit.y, d, v3);
+                        const double vn = std::sqrt(v3[0] * v3[0] + v3[1] * v3[1] + v3[2] * v3[2]);
+                        if (vn > 0.0)
+                            for (int i = 0; i < 3; ++i) o.dir[i] = v3[i] / vn;
+                    } else if (hit.what == bh::Hit::What::Sun) {
+                        const bh::Geom gm = bh::geom_at(cfg.spin, hit.y[bh::Y_R], hit.y[bh::Y_TH]);
+                        const bh::MetricLower ml = bh::metric_lower(gm);
+                        if (ml.tt < 0.0) {
+                            const std::array<double, 4> u = {1.0 / std::sqrt(-ml.tt), 0.0, 0.0, 0.0};
+                            const double g = bh::redshift_factor(hit.y, u);
+                            o.g = (g > 0.0) ? g : 0.0;
+                        }
+                    } else if (hit.what == bh::Hit::What::Star) {
+                        const auto u = cfg.star.surface_four_velocity(hit.y[bh::Y_TH]);
+                        const double ku = hit.y[bh::Y_PT] * u[0] + hit.y[bh::Y_PPH] * u[3];
+                        if (ku > 1e-12) o.g = 1.0 / ku;
+                    }
+                }
+            const double w = 1.0 / (S * S);
+            local.total_flux += acc.y * w;
+        }
+    stats_out(local, st);
+    return BH_OK;
+}
+
+// ---- known-answer quantities (validate.cpp sections 1, 3, 4, 6, 7) --------
+
+void ref_metric_upper_deriv(double a, double r, double th, double out15[15]) {
+    const bh::MetricUpperDeriv d = bh::metric_upper_deriv(a, r, th);
+    const bh::MetricUpper* m[3] = {&d.g, &d.dr, &d.dth};
+    for (int k = 0; k < 3; ++k) {
+        out15[5 * k + 0] = m[k]->tt;
+        out15[5 * k + 1] = m[k]->tp;
+        out15[5 * k + 2] = m[k]->rr;
+        out15[5 * k + 3] = m[k]->thth;
+        out15[5 * k + 4] = m[k]->pp;
+    }
+}
+void ref_metric_lower(double a, double r, double th, double out5[5]) {
+    const bh::MetricLower m = bh::metric_lower(a, r, th);
+    out5[0] = m.tt; out5[1] = m.tp; out5[2] = m.rr; out5[3] = m.thth; out5[4] = m.pp;
+}
+void ref_geodesic_rhs(double a, const double y[8], double dy[8]) {
+    bh::State s;
+    for (int i = 0; i < 8; ++i) s[i] = y[i];
+    const bh::State d = bh::geodesic_rhs(a, s);
+    for (int i = 0; i < 8; ++i) dy[i] = d[i];
+}
+double ref_isco_radius(double a, int sigma) { return bh::isco_radius(a, sigma); }
+double ref_photon_circular_orbit(double a, int sigma) { return bh::photon_circular_orbit(a, sigma); }
+double ref_disc_efficiency(double a, int sigma) { return bh::disc_efficiency(a, sigma); }
+double ref_horizon_outer(double a) { return bh::horizon_outer(a); }
+double ref_page_thorne_W(double a, double r, double r_isco) { return bh::page_thorne_W(a, r, r_isco); }
+double ref_disc_temperature(double M_kg, double spin, double r_out, double eddington, int sense,
+                            double r) {
+    const bh::NovikovThorneDisc d(M_kg, spin, r_out, eddington, sense);
+    return d.temperature(r);
+}
+void ref_blackbody_xyz(double T, double out3[3]) {
+    const spec::XYZ c = spec::blackbody_xyz(T);
+    out3[0] = c.x; out3[1] = c.y; out3[2] = c.z;
+}
+void ref_blackbody_xyz_exact(double T, double out3[3]) {
+    const spec::XYZ c = spec::blackbody_xyz_exact(T);
+    out3[0] = c.x; out3[1] = c.y; out3[2] = c.z;
+}
+void ref_make_photon(double a, double r, double th, double phi, const double dir[3], double y[8]) {
+    const bh::Geom g = bh::geom_at(a, r, th);
+    const bh::Tetrad tet = bh::zamo_tetrad(g);
+    const bh::State s = bh::make_photon(a, r, th, phi, tet, dir, true);
+    for (int i = 0; i < 8; ++i) y[i] = s[i];
+}
+void ref_invariants(double a, const double y[8], double out5[5]) {
+    bh::State s;
+    for (int i = 0; i < 8; ++i) s[i] = y[i];
+    const bh::Invariants iv = bh::invariants(a, s);
+    out5[0] = iv.E; out5[1] = iv.Lz; out5[2] = iv.Q; out5[3] = iv.norm; out5[4] = iv.norm_rel;
+}
+// The star catalogue exactly as StarField builds it (scene.h:62-107).
+int ref_star_catalogue(int count, uint64_t seed, double* out6) {
+    if (count < 0 || !out6) return BH_ERR_INVALID_ARG;
+    const bh::StarField sf(count, seed, true);
+    for (int i = 0; i < count; ++i) {
+        const auto& s = sf.stars_[static_cast<size_t>(i)];
+        double* o = out6 + 6 * static_cast<size_t>(i);
+        o[0] = s.x; o[1] = s.y; o[2] = s.z; o[3] = s.mag; o[4] = s.temperature; o[5] = s.irradiance;
+    }
+    return BH_OK;
+}
+int ref_sky_radiance(int count, uint64_t seed, int milky_way, const double* dirs, int n, double sigma,
+                     double* out3) {
+    const bh::StarField sf(count, seed, milky_way != 0);
+    for (int i = 0; i < n; ++i) {
+        const spec::XYZ c = sf.radiance(dirs + 3 * static_cast<size_t>(i), sigma);
+        out3[3 * i] = c.x; out3[3 * i + 1] = c.y; out3[3 * i + 2] = c.z;
+    }
+    return BH_OK;
+}
+
+}  // extern "C"
