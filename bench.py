@@ -136,25 +136,31 @@ def time_device(r, cfg, steps, warmup, torch, flush, barrier):
     """Average device time of one render (CUDA events on the render stream)."""
     from blackhole_b200 import abi
 
-    stream = torch.cuda.current_stream()
+    # A dedicated (non-default) stream: the kernels, the L2 flush and the
+    # events all go on it, so the events bracket exactly the render's work.
+    stream = torch.cuda.Stream()
     dev = torch.empty((cfg.height, cfg.width, 3), dtype=torch.float64, device="cuda")
     c = cfg.to_c()
-    for _ in range(warmup):
-        r.render_device(c, dev.data_ptr(), stream.cuda_stream)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    barrier()
     torch.cuda.synchronize()
-    for i in range(steps):
-        flush.add_(1.0)
-        starts[i].record(stream)
-        r.render_device(c, dev.data_ptr(), stream.cuda_stream)
-        ends[i].record(stream)
-    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            r.render_device(c, dev.data_ptr(), stream.cuda_stream)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush.add_(1.0)
+            starts[i].record(stream)
+            r.render_device(c, dev.data_ptr(), stream.cuda_stream)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
     barrier()
     times = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     st = abi.bh_render_stats()
     r.render_device(c, dev.data_ptr(), stream.cuda_stream, stats=st)
+    torch.cuda.synchronize()
     return sum(times), times, st, dev
 
 

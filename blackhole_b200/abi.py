@@ -123,6 +123,8 @@ class bh_ray_result(C.Structure):
         ("what", C.c_int32), ("steps", C.c_int32),
         ("y", C.c_double * 8), ("g", C.c_double), ("dir", C.c_double * 3),
         ("xyz", bh_xyz),
+        ("attempts", C.c_int32), ("reserved", C.c_int32),
+        ("max_norm", C.c_double), ("max_q", C.c_double),
     ]
 
 
@@ -139,9 +141,10 @@ def ray_result_dtype():
 
     return np.dtype(
         {
-            "names": ["what", "steps", "y", "g", "dir", "xyz"],
-            "formats": [np.int32, np.int32, (np.float64, 8), np.float64, (np.float64, 3), (np.float64, 3)],
-            "offsets": [0, 4, 8, 72, 80, 104],
+            "names": ["what", "steps", "y", "g", "dir", "xyz", "attempts", "max_norm", "max_q"],
+            "formats": [np.int32, np.int32, (np.float64, 8), np.float64, (np.float64, 3), (np.float64, 3),
+                        np.int32, np.float64, np.float64],
+            "offsets": [0, 4, 8, 72, 80, 104, 128, 136, 144],
             "itemsize": C.sizeof(bh_ray_result),
         }
     )

@@ -955,6 +955,10 @@ __global__ void shade_kernel(ShadeArgs A) {
             o.g = g;
             o.dir[0] = dir[0]; o.dir[1] = dir[1]; o.dir[2] = dir[2];
             o.xyz.x = c[0]; o.xyz.y = c[1]; o.xyz.z = c[2];
+            o.attempts = hr.attempts;
+            o.reserved = 0;
+            o.max_norm = hr.max_norm;
+            o.max_q = hr.max_q;
         }
     }
     const double w = F.inv_SS;

@@ -126,7 +126,8 @@ class Renderer:
     # -- the render path -------------------------------------------------------
     def render(self, cfg, stats: RenderStats | None = None) -> np.ndarray:
         c = _as_c(cfg)
-        out = np.empty((c.height, c.width, 3), dtype=np.float64)
+        # invalid sizes are rejected by the library, not here
+        out = np.empty((max(c.height, 0), max(c.width, 0), 3), dtype=np.float64)
         st = stats.to_c() if stats is not None else abi.bh_render_stats()
         rc = self.lib.bh_gpu_render(self._h, C.byref(c), out.ctypes.data_as(C.POINTER(abi.bh_xyz)),
                                     C.byref(st))

@@ -189,6 +189,10 @@ typedef struct bh_ray_result {
     double g;                /* redshift factor of a disc hit, else 0           */
     double dir[3];           /* unit sky direction of an escaped ray, else 0    */
     bh_xyz xyz;              /* radiance of this sample                          */
+    int32_t attempts;        /* step attempts (accepted + rejected)             */
+    int32_t reserved;
+    double max_norm;         /* worst relative null norm along the ray          */
+    double max_q;            /* worst relative Carter drift along the ray       */
 } bh_ray_result;
 
 /* Launch shape of the persistent trace kernel (the autotuner's search space). */

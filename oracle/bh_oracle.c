@@ -783,7 +783,7 @@ typedef struct {
     double psf_sigma, aspect;
 } scene_t;
 
-typedef struct { int what; double y[8]; double jet; int steps; double q_drift, norm_rel; } hit_t;
+typedef struct { int what; double y[8]; double jet; int steps, attempts; double q_drift, norm_rel; } hit_t;
 
 /* neutronstar.h:94-99 */
 static void ns_surface_four_velocity(const bh_neutron_star* st, double theta, double u[4]) {
@@ -843,8 +843,10 @@ static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* loca
         const double hmax = 0.05 * dmax(1.0, y[YR] - r_h) + 0.01;
         if (h > hmax) h = hmax;
         int tries = 0;
+        ++hit.attempts;
         while (!try_step(&st, y, &h, ynew, &dense)) {
             if (++tries > 40 || fabs(h) < 1e-14) { hit.what = BH_HIT_HORIZON; return hit; }
+            ++hit.attempts;
         }
         ++local->steps;
         ++hit.steps;
@@ -852,6 +854,8 @@ static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* loca
             const invariants_t iv = invariants(a, ynew);
             local->max_norm_error = dmax(local->max_norm_error, fabs(iv.norm_rel));
             local->max_carter_drift = dmax(local->max_carter_drift, fabs(iv.Q - iv0.Q) / Q0);
+            hit.norm_rel = dmax(hit.norm_rel, fabs(iv.norm_rel));
+            hit.q_drift = dmax(hit.q_drift, fabs(iv.Q - iv0.Q) / Q0);
         }
         bl_to_cartesian(a, ynew[YR], ynew[YTH], ynew[YPH], p1);
 
@@ -1136,6 +1140,10 @@ static int run_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                         o->g = g;
                         o->dir[0] = sdir[0]; o->dir[1] = sdir[1]; o->dir[2] = sdir[2];
                         o->xyz.x = c[0]; o->xyz.y = c[1]; o->xyz.z = c[2];
+                        o->attempts = hit.attempts;
+                        o->reserved = 0;
+                        o->max_norm = hit.norm_rel;
+                        o->max_q = hit.q_drift;
                     }
                 }
             }

@@ -256,15 +256,20 @@ int ref_trace_rays(const bh_render_config* c, int x0, int y0, int w, int h, bh_r
                     double dir[3];
                     cfg.cam.ray_direction(u, v, sc.aspect, dir);
                     ++local.rays;
-                    const long long steps0 = local.steps;
-                    const bh::Hit hit = bh::trace(cfg, sc.disc.get(), dir, sc.tet, local);
+                    bh::RenderStats rs;   // this ray's own counters and drift maxima
+                    const bh::Hit hit = bh::trace(cfg, sc.disc.get(), dir, sc.tet, rs);
+                    local.steps += rs.steps;
+                    local.max_norm_error = std::max(local.max_norm_error, rs.max_norm_error);
+                    local.max_carter_drift = std::max(local.max_carter_drift, rs.max_carter_drift);
                     const spec::XYZ col = bh::shade(cfg, sc.disc.get(), sc.stars.get(), hit,
                                                     sc.psf_sigma, sc.jet_colour, local);
                     acc.x += col.x; acc.y += col.y; acc.z += col.z;
                     bh_ray_result& o = out[idx++];
                     std::memset(&o, 0, sizeof o);
                     o.what = static_cast<int32_t>(hit.what);
-                    o.steps = static_cast<int32_t>(local.steps - steps0);
+                    o.steps = static_cast<int32_t>(rs.steps);
+                    o.max_norm = rs.max_norm_error;
+                    o.max_q = rs.max_carter_drift;
                     for (int i = 0; i < 8; ++i) o.y[i] = hit.y[i];
                     o.xyz.x = col.x; o.xyz.y = col.y; o.xyz.z = col.z;
                     // The fields shade_hit computes on the way (render.cpp:275-325).
