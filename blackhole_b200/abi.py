@@ -132,6 +132,7 @@ class bh_launch_params(C.Structure):
     _fields_ = [
         ("block_size", C.c_int32), ("rays_per_thread", C.c_int32),
         ("refill", C.c_int32), ("blocks_per_sm", C.c_int32),
+        ("reg_variant", C.c_int32),
     ]
 
 

@@ -37,7 +37,7 @@ struct bh_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t abort_stream = nullptr;
     std::string err;
-    bh_launch_params launch{128, 1, 16, 0};
+    bh_launch_params launch{128, 1, 32, 0, 1};
     unsigned long long budget = 0;
     std::atomic<int> abort_requested{0};
     int32_t* h_one = nullptr;          // pinned 1, source of the abort copy
@@ -54,7 +54,7 @@ struct bh_ctx {
     int32_t* d_bin_start = nullptr;
     HostSky sky_meta;
 
-    DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats;
+    DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats, deferred;
     QueueState* d_queue = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     long long h2d = 0, d2h = 0;          // bytes copied by the current call
@@ -206,6 +206,9 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     if ((rc = ensure(ctx, ctx->partials, static_cast<size_t>(n) * kReduceBlocks * sizeof(FrameStats))) != BH_OK)
         return rc;
     if ((rc = ensure(ctx, ctx->fstats, n * sizeof(FrameStats))) != BH_OK) return rc;
+    const bool mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
+    if (mixed && (rc = ensure(ctx, ctx->deferred, static_cast<size_t>(rays) * deferred_record_bytes())) != BH_OK)
+        return rc;
 
     CK(cudaMemcpyAsync(ctx->frames.p, frames.data(), n * sizeof(FrameParams), cudaMemcpyHostToDevice, stream));
     CK(cudaMemcpyAsync(ctx->ray_end.p, ray_end.data(), n * sizeof(long long), cudaMemcpyHostToDevice, stream));
@@ -219,7 +222,7 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
 
     const bh_launch_params& lp = ctx->launch;
     const int prec = frames[0].precision_tag;
-    int bps = lp.blocks_per_sm > 0 ? lp.blocks_per_sm : trace_blocks_per_sm(prec, lp.block_size);
+    int bps = lp.blocks_per_sm > 0 ? lp.blocks_per_sm : trace_blocks_per_sm(prec, lp.block_size, lp.reg_variant == 2);
     if (bps < 1) bps = 1;
     TraceLaunch tl;
     tl.frames = static_cast<const FrameParams*>(ctx->frames.p);
@@ -234,6 +237,13 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     tl.rays_per_thread = lp.rays_per_thread;
     tl.refill = lp.refill;
     tl.budget = ctx->budget;
+    tl.deferred = mixed ? ctx->deferred.p : nullptr;
+    tl.reg_variant = (lp.reg_variant == 2) ? 1 : 0;
+    {
+        int bps64 = trace_blocks_per_sm(BH_PRECISION_FP64, lp.block_size, lp.reg_variant == 2);
+        tl.grid_resume = ctx->sm_count * (bps64 < 1 ? 1 : bps64);
+    }
+    tl.resume_event = timed ? ctx->ev[3] : nullptr;
     if (timed) CK(cudaEventRecord(ctx->ev[0], stream));
     if (rays > 0) CK(launch_trace(tl, stream));
     if (timed) CK(cudaEventRecord(ctx->ev[1], stream));
@@ -373,7 +383,7 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end,
+    for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end, &ctx->deferred,
                       &ctx->pix_end, &ctx->partials, &ctx->fstats})
         if (b->p) cudaFree(b->p);
     cudaFree(ctx->d_table);
@@ -517,6 +527,15 @@ int bh_gpu_set_launch(bh_ctx* ctx, const bh_launch_params* p) {
             return fail(ctx, BH_ERR_INVALID_ARG, "blocks_per_sm must be in [0, 64]");
         n.blocks_per_sm = p->blocks_per_sm;
     }
+    if (p->reg_variant) {
+        if (p->reg_variant != 1 && p->reg_variant != 2)
+            return fail(ctx, BH_ERR_INVALID_ARG, "reg_variant must be 1 (tight) or 2 (wide)");
+        n.reg_variant = p->reg_variant;
+    }
+    // Threads x registers of one block must fit in the SM's 64 K registers.
+    const int prec_max = (n.reg_variant == 2) ? 232 : 168;
+    if (n.block_size * prec_max > 65536)
+        return fail(ctx, BH_ERR_INVALID_ARG, "block_size too large for the register cap of the binary64 kernel");
     ctx->launch = n;
     return BH_OK;
 }

@@ -22,6 +22,7 @@ struct FrameParams {
     double r_escape;
     double rtol, atol;               // tolerances of this frame's precision
     double h0;                       // first trial step, 0.02 max(1, r_cam) (render.cpp:86)
+    double r_promote;                // innermost photon orbit: an ingoing ray below it is falling in
     int32_t max_steps;
     int32_t factored_delta;          // Delta = (r - r+)(r - r-) when a^2 < 1
 
@@ -115,8 +116,10 @@ struct QueueState {
     unsigned long long next;         // next unclaimed global ray id
     unsigned long long attempts;     // step attempts of finished rays
     unsigned long long budget;       // 0 = none
-    int32_t abort;                   // set by the host or by the budget check
-    int32_t status;                  // 0 ok, 1 aborted, 2 budget
+    unsigned long long deferred;     // rays handed from binary32 to binary64
+    unsigned long long resume_next;  // next unclaimed deferred ray
+    int32_t abort;                   // set by the host (1) or by the budget check (2)
+    int32_t status;
 };
 
 }  // namespace bhg

@@ -23,15 +23,22 @@ struct TraceLaunch {
     int rays_per_thread;
     int refill;
     unsigned long long budget;       // step-attempt budget of the launch, 0 = none
+    int reg_variant;                 // 0: default register cap, 1: the wider one
+    void* deferred;                  // mixed precision: total_rays deferred records
+    int grid_resume;                 // blocks of the binary64 resume launch
+    cudaEvent_t resume_event;        // recorded between the two launches (optional)
 };
+
+// Bytes of one deferred-ray record.
+size_t deferred_record_bytes();
 
 // Persistent trace kernel over all rays of all frames.
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream);
 
 // Blocks per SM that fit for a precision and block size (occupancy query).
-int trace_blocks_per_sm(int precision, int block_size);
+int trace_blocks_per_sm(int precision, int block_size, int variant);
 // Registers per thread of the trace kernel of a precision (for reports).
-int trace_registers(int precision);
+int trace_registers(int precision, int variant);
 
 struct ShadeLaunch {
     const FrameParams* frames;

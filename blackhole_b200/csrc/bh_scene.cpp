@@ -299,6 +299,10 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     F.rtol = rtol;
     F.atol = atol;
     F.h0 = 0.02 * maxd(1.0, c.cam.r);
+    // Innermost (prograde equatorial) photon orbit, kerr.h:217-220 with |a|:
+    // a photon from far away that is moving inwards below it has no radial
+    // turning point left and falls into the hole.
+    F.r_promote = (F.a2 < 1.0) ? 2.0 * (1.0 + std::cos((2.0 / 3.0) * std::acos(-std::fabs(a)))) : 0.0;
     F.max_steps = c.max_steps;
 
     // Camera (scene.h:356-384, render.cpp:409-414).

@@ -1,0 +1,763 @@
+// bh_trace.cu - The persistent trace kernels of the render path (sm_100a).
+//
+//   trace_kernel<Fp64>   every operation in binary64.
+//   trace_kernel<Mixed>  binary32 ray state, stages and right-hand side;
+//                        binary64 for the step size, the error-norm sum and
+//                        the accept/reject test, event root refinement and the
+//                        invariant diagnostics.  A ray that is provably falling
+//                        into the hole (moving inwards inside the innermost
+//                        photon orbit) is handed to binary64 for the plunge,
+//                        where Delta -> 0 makes the binary32 Hamiltonian lose
+//                        all its digits: its state goes to a deferred list and
+//                        trace_kernel<Fp64> resumes it in a second launch.
+//
+// Each lane integrates one ray: ray set-up (render.cpp:440-451,
+// geodesic.h:215-231), DP5(4) attempts with PI step control
+// (geodesic.h:123-204) under the hmax limiter (render.cpp:130-131), the
+// invariant diagnostics (render.cpp:139-145) and the events (render.cpp:158-251).
+// A warp refills lanes freed by terminated rays from a global atomic queue:
+// one atomicAdd per refill, new ids compacted over the idle lanes with
+// ballot/popc, so a refill hands out a contiguous (image-coherent) run of rays.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/bh_gpu.h"
+#include "bh_common.cuh"
+#include "bh_frame.h"
+#include "bh_launch.h"
+
+namespace bhg {
+
+namespace {
+
+// ---- Dormand-Prince 5(4) (Hairer, Norsett & Wanner, Solving ODEs I, II.4) ----
+constexpr double A21 = 1.0 / 5.0;
+constexpr double A31 = 3.0 / 40.0, A32 = 9.0 / 40.0;
+constexpr double A41 = 44.0 / 45.0, A42 = -56.0 / 15.0, A43 = 32.0 / 9.0;
+constexpr double A51 = 19372.0 / 6561.0, A52 = -25360.0 / 2187.0, A53 = 64448.0 / 6561.0,
+                 A54 = -212.0 / 729.0;
+constexpr double A61 = 9017.0 / 3168.0, A62 = -355.0 / 33.0, A63 = 46732.0 / 5247.0,
+                 A64 = 49.0 / 176.0, A65 = -5103.0 / 18656.0;
+constexpr double B1 = 35.0 / 384.0, B3 = 500.0 / 1113.0, B4 = 125.0 / 192.0,
+                 B5 = -2187.0 / 6784.0, B6 = 11.0 / 84.0;
+constexpr double E1 = 35.0 / 384.0 - 5179.0 / 57600.0;
+constexpr double E3 = 500.0 / 1113.0 - 7571.0 / 16695.0;
+constexpr double E4 = 125.0 / 192.0 - 393.0 / 640.0;
+constexpr double E5 = -2187.0 / 6784.0 - (-92097.0 / 339200.0);
+constexpr double E6 = 11.0 / 84.0 - 187.0 / 2100.0;
+constexpr double E7 = 0.0 - 1.0 / 40.0;
+constexpr double D1 = -12715105075.0 / 11282082432.0, D3 = 87487479700.0 / 32700410799.0,
+                 D4 = -10690763975.0 / 1880347072.0, D5 = 701980252875.0 / 199316789632.0,
+                 D6 = -1453857185.0 / 822651844.0, D7 = 69997945.0 / 29380423.0;
+// PI controller (Gustafsson): alpha = 0.7/5, beta = 0.4/5, safety 0.9, [0.2, 5].
+constexpr double kAlpha = 0.7 / 5.0, kBeta = 0.4 / 5.0;
+
+// ---- precision policies -------------------------------------------------------
+struct Fp64 {
+    using R = double;
+    static constexpr bool kMixed = false;
+    __device__ static __forceinline__ void sc(double x, double* s, double* c) { sincos(x, s, c); }
+    __device__ static __forceinline__ double rcp(double x) { return 1.0 / x; }
+    __device__ static __forceinline__ double powd(double x, double y) { return pow(x, y); }
+};
+
+struct Mixed {
+    using R = float;
+    static constexpr bool kMixed = true;
+    __device__ static __forceinline__ void sc(float x, float* s, float* c) { sincosf(x, s, c); }
+    __device__ static __forceinline__ float rcp(float x) {
+        float r;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+        return r;
+    }
+    __device__ static __forceinline__ double powd(double x, double y) {
+        return (double)__powf((float)x, (float)y);
+    }
+};
+
+// Exact (non-contracted) binary64 arithmetic for the ray set-up, so that the
+// initial photon reproduces the host (reference) computation bit for bit.
+__device__ __forceinline__ double xm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xa(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b); }
+
+// Initial photon state of frame-local ray `local_id` (render.cpp:440-451,
+// scene.h:356-384, geodesic.h:215-231) and its Carter constant
+// (kerr.h:342-348, with the camera's sin^2/cos^2 precomputed on the host).
+__device__ void ray_setup(const FrameParams& F, long long local_id, double y[8], double* Q0) {
+    const int S = F.S;
+    const long long pixel = local_id / (S * S);
+    const int k = (int)(local_id - pixel * (S * S));
+    const int sy = k / S, sx = k - (k / S) * S;
+    int px, py;
+    pixel_xy(F.width, F.height, pixel, &px, &py);
+    // Rng(seed ^ y<<32 ^ x*phi64), draws 2k+1 and 2k+2 of its splitmix64 stream.
+    const uint64_t s0 = F.seed ^ ((uint64_t)py << 32) ^ ((uint64_t)px * 0x9E3779B97F4A7C15ull);
+    const uint64_t g = 0x9E3779B97F4A7C15ull;
+    const double u1 = u53(mix64(s0 + (uint64_t)(2 * k + 1) * g));
+    const double u2 = u53(mix64(s0 + (uint64_t)(2 * k + 2) * g));
+    const double jx = xm(xa((double)sx, u1), F.inv_S);
+    const double jy = xm(xa((double)sy, u2), F.inv_S);
+    const double su = xs(__ddiv_rn(xm(2.0, xa((double)px, jx)), (double)F.width), 1.0);
+    const double sv = xs(1.0, __ddiv_rn(xm(2.0, xa((double)py, jy)), (double)F.height));
+    double x = xm(su, F.tanf);
+    double yy = __ddiv_rn(xm(sv, F.tanf), F.aspect);
+    const double z = 1.0;
+    if (F.has_roll) {
+        const double xr = xs(xm(F.cr, x), xm(F.sr, yy));
+        const double yr = xa(xm(F.sr, x), xm(F.cr, yy));
+        x = xr; yy = yr;
+    }
+    const double y2 = xs(xm(F.cp, yy), xm(F.sp, z));
+    const double z2 = xa(xm(F.sp, yy), xm(F.cp, z));
+    const double x2 = xa(xm(F.cy, x), xm(F.sy, z2));
+    const double z3 = xa(xm(-F.sy, x), xm(F.cy, z2));
+    const double v0 = -z3, v1 = -y2, v2 = x2;
+    const double n = __dsqrt_rn(xa(xa(xm(v0, v0), xm(v1, v1)), xm(v2, v2)));
+    const double d0 = __ddiv_rn(v0, n), d1 = __ddiv_rn(v1, n), d2 = __ddiv_rn(v2, n);
+    // p^mu = -(e_0 - d^i e_i) with the ZAMO legs, then lowered with g_{mu nu}.
+    const double zero = 0.0;
+    const double p0 = -xa(F.tet00, xm(-1.0, xa(xa(xm(d0, zero), xm(d1, zero)), xm(d2, zero))));
+    const double p1 = -xa(zero, xm(-1.0, xa(xa(xm(d0, F.tet11), xm(d1, zero)), xm(d2, zero))));
+    const double p2 = -xa(zero, xm(-1.0, xa(xa(xm(d0, zero), xm(d1, F.tet22)), xm(d2, zero))));
+    const double p3 = -xa(F.tet03, xm(-1.0, xa(xa(xm(d0, zero), xm(d1, zero)), xm(d2, F.tet33))));
+    y[0] = 0.0;
+    y[1] = F.cam_r;
+    y[2] = F.cam_th;
+    y[3] = F.cam_ph;
+    y[4] = xa(xm(F.ml_tt, p0), xm(F.ml_tp, p3));
+    y[5] = xm(F.ml_rr, p1);
+    y[6] = xm(F.ml_thth, p2);
+    y[7] = xa(xm(F.ml_tp, p0), xm(F.ml_pp, p3));
+    const double E = -y[4], Lz = y[7], pth = y[6];
+    *Q0 = xa(xm(pth, pth), xm(F.cam_cs2, xa(xm(xm(F.a, F.a), xs(0.0, xm(E, E))),
+                                              __ddiv_rn(xm(Lz, Lz), F.cam_sn2))));
+}
+
+// ---- lane state -------------------------------------------------------------
+template <class P>
+struct Lane {
+    using R = typename P::R;
+    R y[6];                  // t, r, th, phi, p_r, p_th
+    R k1[6];                 // FSAL stage
+    R E, Lz, aR, a2R, aE, aLz, a2E2, Lz2;
+    R rp_hi, rp_lo, rm_hi, rm_lo;   // r_+ and r_- as exact two-term sums
+    R c0;                    // cos(th) at y, for the disc-plane test
+    double h;
+    R err_prev, errp_pow;    // PI-controller memory and pow(err_prev, beta)
+    double Q0;
+    float inv_Q0, max_norm, max_q;
+    int steps, tries, attempts;
+    int att0;                // attempts already counted against the budget
+    int gid, frame;
+    int have_k1;
+    int factored;
+    int bad_sc;
+};
+
+template <class P>
+struct Aux {
+    typename P::R cs, sn2, cs2, D;
+};
+
+// Hamilton's equations for H = 1/2 g^{mu nu} p_mu p_nu (geodesic.h:50-71),
+// with the Kerr inverse metric in Carter's separated form
+//   2 Sigma H = Delta p_r^2 + p_th^2 + (L_z - a E sin^2)^2 / sin^2
+//               - ((r^2 + a^2) E - a L_z)^2 / Delta,
+// E = -p_t and L_z = p_phi constant (their derivatives vanish exactly).  The
+// same function of (r, th, p) as the reference's quotient-rule form; three
+// reciprocals instead of fifteen divisions.  H = 0 is not imposed (B is the
+// full bracket).  Delta = (r - r_+)(r - r_-) with each factor formed against
+// a two-term r_+-, so the factor that vanishes at the horizon is exact.
+template <class P>
+__device__ __forceinline__ void rhs(const Lane<P>& L, typename P::R r, typename P::R th,
+                                    typename P::R pr, typename P::R pth, typename P::R* d,
+                                    Aux<P>* aux) {
+    using R = typename P::R;
+    R sn, cs;
+    P::sc(th, &sn, &cs);
+    if (fabs(sn) < R(1e-9)) sn = (sn < R(0)) ? R(-1e-9) : R(1e-9);   // kerr.h:51
+    const R sn2 = sn * sn, cs2 = cs * cs;
+    const R r2 = r * r;
+    const R S = r2 + L.a2R * cs2;
+    const R D = L.factored ? ((r - L.rp_hi) - L.rp_lo) * ((r - L.rm_hi) - L.rm_lo)
+                           : (r2 - R(2) * r + L.a2R);
+    const R iS = P::rcp(S), iD = P::rcp(D), isn2 = P::rcp(sn2);
+    const R r2a2 = r2 + L.a2R;
+    const R K = r2a2 * L.E - L.aLz;
+    const R Lp = L.Lz - L.aE * sn2;
+    const R KiD = K * iD;
+    const R B = D * pr * pr + pth * pth + Lp * Lp * isn2 - K * KiD;
+    const R Dr = R(2) * r - R(2);
+    d[0] = iS * (L.aR * Lp + r2a2 * KiD);
+    d[1] = D * pr * iS;
+    d[2] = pth * iS;
+    d[3] = iS * (Lp * isn2 + L.aR * KiD);
+    d[4] = R(-0.5) * iS * (Dr * pr * pr - R(4) * r * L.E * KiD + Dr * KiD * KiD - R(2) * r * B * iS);
+    d[5] = -sn * cs * iS * (L.a2E2 - L.Lz2 * isn2 * isn2 + L.a2R * B * iS);
+    if (aux) {
+        aux->cs = cs;
+        aux->sn2 = sn2;
+        aux->cs2 = cs2;
+        aux->D = D;
+    }
+}
+
+// Dense-output polynomial of one component (geodesic.h:109-121, 176-185).
+struct DenseC { double r1, r2, r3, r4, r5; };
+
+__device__ __forceinline__ DenseC dense_coef(double h, double y, double yn, double k1, double k3,
+                                             double k4, double k5, double k6, double k7) {
+    DenseC c;
+    c.r1 = y;
+    c.r2 = yn - y;
+    c.r3 = h * k1 - c.r2;
+    c.r4 = c.r2 - h * k7 - c.r3;
+    c.r5 = h * (D1 * k1 + D3 * k3 + D4 * k4 + D5 * k5 + D6 * k6 + D7 * k7);
+    return c;
+}
+__device__ __forceinline__ double dense_eval(const DenseC& c, double s) {
+    const double s1 = 1.0 - s;
+    return c.r1 + s * (c.r2 + s1 * (c.r3 + s * (c.r4 + s1 * c.r5)));
+}
+__device__ __forceinline__ double dense_deriv(const DenseC& c, double s) {
+    const double u = 1.0 - s;
+    return c.r2 + (u - s) * c.r3 + (2.0 * s * u - s * s) * c.r4 + (2.0 * s * u * u - 2.0 * s * s * u) * c.r5;
+}
+
+// Crossing of `target` by the dense polynomial on [0, 1]: safeguarded Newton
+// inside a shrinking bracket.  It converges to the same point (to rounding) as
+// the reference's 60-step bisection on the same polynomial (render.cpp:158-166,
+// 181-189), in a handful of binary64 evaluations.  f(0) <= 0 -> s = 0.
+__device__ double dense_crossing(const DenseC& c, double target) {
+    double lo = 0.0, hi = 1.0;
+    const double f0 = c.r1 - target;
+    const double f1 = (c.r1 + c.r2) - target;
+    if (f0 == 0.0) return 0.0;
+    if (f1 == 0.0 || !((f0 < 0.0) != (f1 < 0.0))) {
+        // no bracket (the crossing and back inside one step): plain bisection
+        // on the sign at s = 0, as the reference does
+        for (int it = 0; it < 60; ++it) {
+            const double mid = 0.5 * (lo + hi);
+            if (((dense_eval(c, mid) - target) < 0.0) != (f0 < 0.0)) hi = mid; else lo = mid;
+        }
+        return 0.5 * (lo + hi);
+    }
+    const bool neg0 = f0 < 0.0;
+    double s = f0 / (f0 - f1);
+    for (int it = 0; it < 50; ++it) {
+        const double f = dense_eval(c, s) - target;
+        if (f == 0.0) return s;
+        if ((f < 0.0) == neg0) lo = s; else hi = s;
+        const double d = dense_deriv(c, s);
+        double sn = s - f / d;
+        if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
+        if (fabs(sn - s) <= 4e-16 || hi - lo <= 4e-16) return sn;
+        s = sn;
+    }
+    return s;
+}
+
+// Deferred ray: a mixed-precision ray handed to the binary64 kernel.
+struct Deferred {
+    double y[6];
+    double h;
+    double Q0;
+    float err_prev, max_norm, max_q;
+    int gid, frame, steps, attempts, pad;
+};
+
+struct TraceArgs {
+    const FrameParams* frames;
+    const long long* frame_ray_end;
+    int nframes;
+    long long total_rays;
+    HitRecord* hits;
+    QueueState* queue;
+    Deferred* deferred;      // mixed: append target; resume: source
+    int resume;              // 1: take rays from the deferred list
+    int rays_per_thread;
+    int refill;
+    unsigned long long budget;
+};
+
+template <class P>
+__device__ __forceinline__ void state8(const Lane<P>& L, const double ptph[2], double y8[8]) {
+    y8[0] = (double)L.y[0];
+    y8[1] = (double)L.y[1];
+    y8[2] = (double)L.y[2];
+    y8[3] = (double)L.y[3];
+    y8[4] = ptph[0];
+    y8[5] = (double)L.y[4];
+    y8[6] = (double)L.y[5];
+    y8[7] = ptph[1];
+}
+
+template <class P>
+__device__ __forceinline__ void write_hit(const TraceArgs& A, const Lane<P>& L, int what, const double y8[8]) {
+    // y[4] = p_t and y[7] = p_phi were stored exactly when the ray started.
+    HitRecord* o = &A.hits[L.gid];
+    o->y[0] = y8[0];
+    o->y[1] = y8[1];
+    o->y[2] = y8[2];
+    o->y[3] = y8[3];
+    o->y[5] = y8[5];
+    o->y[6] = y8[6];
+    o->max_norm = (double)L.max_norm;
+    o->max_q = (double)L.max_q;
+    o->what = what;
+    o->steps = L.steps;
+    o->attempts = L.attempts;
+}
+
+// Lane set-up from an initial photon (fresh ray) or a deferred state.
+template <class P>
+__device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
+    using R = typename P::R;
+    const Deferred* dr = nullptr;
+    if (A.resume) {
+        dr = &A.deferred[id];
+        L.gid = dr->gid;
+        L.frame = dr->frame;
+    } else {
+        L.gid = (int)id;
+        L.frame = find_frame(A.frame_ray_end, A.nframes, id);
+    }
+    const FrameParams& F = A.frames[L.frame];
+    double y8[8], Q0;
+    ray_setup(F, (long long)L.gid - F.ray_begin, y8, &Q0);
+    const double E = -y8[4], Lz = y8[7];
+    L.E = (R)E;
+    L.Lz = (R)Lz;
+    L.aR = (R)F.a;
+    L.a2R = (R)F.a2;
+    L.aE = (R)(F.a * E);
+    L.aLz = (R)(F.a * Lz);
+    L.a2E2 = (R)(F.a2 * E * E);
+    L.Lz2 = (R)(Lz * Lz);
+    L.rp_hi = (R)F.r_plus;
+    L.rp_lo = (R)(F.r_plus - (double)L.rp_hi);
+    L.rm_hi = (R)F.r_minus;
+    L.rm_lo = (R)(F.r_minus - (double)L.rm_hi);
+    L.factored = F.factored_delta;
+    L.bad_sc = (F.atol + F.rtol * fabs(y8[4]) == 0.0) || (F.atol + F.rtol * fabs(y8[7]) == 0.0);
+    L.tries = 0;
+    L.have_k1 = 0;
+    // p_t and p_phi never change: store them now, the rest at termination.
+    A.hits[L.gid].y[4] = y8[4];
+    A.hits[L.gid].y[7] = y8[7];
+    if (dr) {
+        #pragma unroll
+        for (int i = 0; i < 6; ++i) L.y[i] = (R)dr->y[i];
+        L.h = dr->h;
+        L.err_prev = (R)dr->err_prev;
+        L.Q0 = dr->Q0;
+        L.max_norm = dr->max_norm;
+        L.max_q = dr->max_q;
+        L.steps = dr->steps;
+        L.attempts = dr->attempts;
+        L.att0 = dr->attempts;
+    } else {
+        L.y[0] = (R)y8[0]; L.y[1] = (R)y8[1]; L.y[2] = (R)y8[2]; L.y[3] = (R)y8[3];
+        L.y[4] = (R)y8[5]; L.y[5] = (R)y8[6];
+        L.h = F.h0;
+        L.err_prev = R(1e-4);
+        if (P::kMixed) {
+            // Carter constant of the binary32 initial state, the reference for
+            // the drift of the binary32 integration.
+            const double cs2 = F.cam_cs2, sn2 = F.cam_sn2;
+            const double Ef = (double)L.E, Lf = (double)L.Lz, pf = (double)L.y[5];
+            L.Q0 = pf * pf + cs2 * (F.a2 * (0.0 - Ef * Ef) + Lf * Lf / sn2);
+        } else {
+            L.Q0 = Q0;
+        }
+        L.max_norm = 0.f;
+        L.max_q = 0.f;
+        L.steps = 0;
+        L.attempts = 0;
+        L.att0 = 0;
+    }
+    L.errp_pow = (R)P::powd(dmaxr((double)L.err_prev, 1e-4), kBeta);
+    L.inv_Q0 = (float)(1.0 / (fabs(L.Q0) + 1e-12));
+    if (!dr && F.max_steps <= 0) {
+        write_hit(A, L, BH_HIT_EXHAUSTED, y8);
+        return false;
+    }
+    return true;
+}
+
+// One step attempt.  Returns true when the lane's ray is finished here
+// (terminated, or deferred to the binary64 kernel).
+template <class P>
+__device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
+    using R = typename P::R;
+    const FrameParams& F = A.frames[L.frame];
+    if (L.tries == 0) {
+        const double hmax = 0.05 * dmaxr(1.0, (double)L.y[1] - F.r_h) + 0.01;
+        if (L.h > hmax) L.h = hmax;
+    }
+    if (!L.have_k1) {
+        Aux<P> ax;
+        rhs<P>(L, L.y[1], L.y[2], L.y[4], L.y[5], L.k1, &ax);
+        L.c0 = ax.cs;
+        L.have_k1 = 1;
+    }
+    const R h = (R)L.h;
+    R t[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], yn[6];
+    #pragma unroll
+    for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * R(A21) * L.k1[i];
+    rhs<P>(L, t[1], t[2], t[4], t[5], k2, nullptr);
+    #pragma unroll
+    for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * (R(A31) * L.k1[i] + R(A32) * k2[i]);
+    rhs<P>(L, t[1], t[2], t[4], t[5], k3, nullptr);
+    #pragma unroll
+    for (int i = 0; i < 6; ++i)
+        t[i] = L.y[i] + h * (R(A41) * L.k1[i] + R(A42) * k2[i] + R(A43) * k3[i]);
+    rhs<P>(L, t[1], t[2], t[4], t[5], k4, nullptr);
+    #pragma unroll
+    for (int i = 0; i < 6; ++i)
+        t[i] = L.y[i] + h * (R(A51) * L.k1[i] + R(A52) * k2[i] + R(A53) * k3[i] + R(A54) * k4[i]);
+    rhs<P>(L, t[1], t[2], t[4], t[5], k5, nullptr);
+    #pragma unroll
+    for (int i = 0; i < 6; ++i)
+        t[i] = L.y[i] + h * (R(A61) * L.k1[i] + R(A62) * k2[i] + R(A63) * k3[i] +
+                             R(A64) * k4[i] + R(A65) * k5[i]);
+    rhs<P>(L, t[1], t[2], t[4], t[5], k6, nullptr);
+    #pragma unroll
+    for (int i = 0; i < 6; ++i)
+        yn[i] = L.y[i] + h * (R(B1) * L.k1[i] + R(B3) * k3[i] + R(B4) * k4[i] + R(B5) * k5[i] +
+                              R(B6) * k6[i]);
+    Aux<P> ax7;
+    rhs<P>(L, yn[1], yn[2], yn[4], yn[5], k7, &ax7);
+
+    // RMS error over the eight components (geodesic.h:157-166): the p_t and
+    // p_phi terms are exactly zero.  Squares summed in binary64.
+    double err2 = 0.0;
+    #pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const R e = h * (R(E1) * L.k1[i] + R(E3) * k3[i] + R(E4) * k4[i] + R(E5) * k5[i] +
+                         R(E6) * k6[i] + R(E7) * k7[i]);
+        if (P::kMixed) {
+            const float sc = (float)F.atol + (float)F.rtol * fmaxf(fabsf((float)L.y[i]), fabsf((float)yn[i]));
+            const float q = (float)e * Mixed::rcp(sc);
+            err2 += (double)q * (double)q;
+        } else {
+            const double sc = F.atol + F.rtol * dmaxr(fabs((double)L.y[i]), fabs((double)yn[i]));
+            const double q = (double)e / sc;
+            err2 += q * q;
+        }
+    }
+    double err = sqrt(err2 / 8.0);
+    if (L.bad_sc || !isfinite(err)) err = 1e10;
+    ++L.attempts;
+    double fac = 0.9 * P::powd(dmaxr(err, 1e-16), -kAlpha) * (double)L.errp_pow;
+    fac = dclamp(fac, 0.2, 5.0);
+
+    if (!(err <= 1.0)) {
+        L.h *= dminr(fac, 1.0);
+        if (++L.tries > 40 || fabs(L.h) < 1e-14) {
+            // render.cpp:133-136: no acceptable step is a capture, reported
+            // with the ray's initial state.
+            double y8[8], Q0;
+            ray_setup(F, (long long)L.gid - F.ray_begin, y8, &Q0);
+            write_hit(A, L, BH_HIT_HORIZON, y8);
+            return true;
+        }
+        return false;
+    }
+
+    // ---- accepted -----------------------------------------------------------
+    L.tries = 0;
+    ++L.steps;
+    const double rn = (double)yn[1];
+    const double pt = -(double)L.E, pph = (double)L.Lz;
+    {
+        // Invariant diagnostics at y_new (render.cpp:139-145) in binary64.
+        // The five terms of g^{ab} p_a p_b (kerr.h:301-321) are all scaled by
+        // Sigma Delta sin^2 > 0 and Carter's Q by sin^2, which leaves both
+        // ratios unchanged; a division only when a maximum grows.
+        const double sn2 = (double)ax7.sn2, cs2 = (double)ax7.cs2, Del = (double)ax7.D;
+        const double pr = (double)yn[4], pth = (double)yn[5];
+        const double a2 = F.a2;
+        const double rpa = rn * rn + a2;
+        const double Ak = rpa * rpa - a2 * Del * sn2;
+        const double T1 = -Ak * pt * pt * sn2;
+        const double T2 = -4.0 * F.a * rn * pt * pph * sn2;
+        const double T3 = Del * Del * sn2 * pr * pr;
+        const double T4 = Del * sn2 * pth * pth;
+        const double T5 = (Del - a2 * sn2) * pph * pph;
+        const double nrm = fabs(T1 + T2 + T3 + T4 + T5);
+        const double scl = fabs(T1) + fabs(T2) + fabs(T3) + fabs(T4) + fabs(T5);
+        if (nrm > (double)L.max_norm * scl) L.max_norm = (float)((scl > 0.0) ? nrm / scl : nrm);
+        const double Qs = pth * pth * sn2 + cs2 * (a2 * (0.0 - pt * pt) * sn2 + pph * pph);
+        const double dev = fabs(Qs - L.Q0 * sn2) * (double)L.inv_Q0;
+        if (dev > (double)L.max_q * sn2) L.max_q = (float)(dev / sn2);
+    }
+
+    const double hd = L.h;
+    const double ptph[2] = {pt, pph};
+    int what = -1;
+    double yh[8];
+    auto dense_state = [&](double s_end) {
+        #pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const DenseC c = dense_coef(hd, L.y[i], yn[i], L.k1[i], k3[i], k4[i], k5[i], k6[i], k7[i]);
+            yh[i < 4 ? i : i + 1] = dense_eval(c, s_end);
+        }
+        yh[4] = pt;
+        yh[7] = pph;
+    };
+    if (F.ns_enabled && rn <= F.ns_R) {
+        // neutron-star surface (render.cpp:158-169)
+        const DenseC cr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
+        what = BH_HIT_STAR;
+        dense_state(dense_crossing(cr, F.ns_R));
+    } else if (rn <= F.r_stop) {
+        what = BH_HIT_HORIZON;             // render.cpp:172-177
+    } else if (F.disc_enabled && (double)L.c0 * (double)ax7.cs < 0.0) {
+        // equatorial crossing (render.cpp:180-199): cos(th) changes sign at
+        // th* = pi/2 + m pi between th(0) and th(1)
+        const DenseC cth = dense_coef(hd, L.y[2], yn[2], L.k1[2], k3[2], k4[2], k5[2], k6[2], k7[2]);
+        const double th0 = cth.r1, th1 = cth.r1 + cth.r2;
+        const double m = (th1 > th0) ? ceil((th0 - 0.5 * kPi) / kPi) : floor((th0 - 0.5 * kPi) / kPi);
+        const double s_end = dense_crossing(cth, 0.5 * kPi + m * kPi);
+        const DenseC crr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
+        const double rc = dense_eval(crr, s_end);
+        if (rc >= F.r_in && rc <= F.r_out) {
+            what = BH_HIT_DISC;
+            dense_state(s_end);
+        }
+    }
+    if (what < 0 && F.sun_enabled) {
+        // The Sun (render.cpp:201-241): probe the dense geodesic, then bisect.
+        const double a = F.a;
+        auto cart = [&](double r, double th, double ph, double q[3]) {
+            const double rr = sqrt(r * r + a * a);
+            const double sn = sin(th);
+            q[0] = rr * sn * cos(ph);
+            q[1] = rr * sn * sin(ph);
+            q[2] = r * cos(th);
+        };
+        double p0[3], p1[3];
+        cart((double)L.y[1], (double)L.y[2], (double)L.y[3], p0);
+        cart(rn, (double)yn[2], (double)yn[3], p1);
+        const double sg0 = p1[0] - p0[0], sg1 = p1[1] - p0[1], sg2 = p1[2] - p0[2];
+        const double seg_len = sqrt(sg0 * sg0 + sg1 * sg1 + sg2 * sg2);
+        const double dc = sqrt((p0[0] - F.sun_c[0]) * (p0[0] - F.sun_c[0]) +
+                               (p0[1] - F.sun_c[1]) * (p0[1] - F.sun_c[1]) +
+                               (p0[2] - F.sun_c[2]) * (p0[2] - F.sun_c[2]));
+        if (dc <= seg_len + F.sun_R * 1.5) {
+            const DenseC cr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
+            const DenseC ct = dense_coef(hd, L.y[2], yn[2], L.k1[2], k3[2], k4[2], k5[2], k6[2], k7[2]);
+            const DenseC cp = dense_coef(hd, L.y[3], yn[3], L.k1[3], k3[3], k4[3], k5[3], k6[3], k7[3]);
+            auto f = [&](double s) {
+                double q[3];
+                cart(dense_eval(cr, s), dense_eval(ct, s), dense_eval(cp, s), q);
+                const double dx = q[0] - F.sun_c[0], dy = q[1] - F.sun_c[1], dz = q[2] - F.sun_c[2];
+                return dx * dx + dy * dy + dz * dz - F.sun_R2;
+            };
+            if (f(0.0) <= 0.0) {
+                what = BH_HIT_SUN;
+                state8(L, ptph, yh);       // already inside at the start of the step
+            } else {
+                double prev_s = 0.0;
+                for (int k = 1; k <= 12; ++k) {
+                    const double s = (double)k / 12;
+                    if (f(s) <= 0.0) {
+                        double lo = prev_s, hi = s;
+                        for (int b = 0; b < 50; ++b) {
+                            const double mid = 0.5 * (lo + hi);
+                            if (f(mid) <= 0.0) hi = mid; else lo = mid;
+                        }
+                        what = BH_HIT_SUN;
+                        dense_state(0.5 * (lo + hi));
+                        break;
+                    }
+                    prev_s = s;
+                }
+            }
+        }
+    }
+    if (what < 0 && rn > F.r_escape) what = BH_HIT_SKY;   // render.cpp:247-251
+
+    // Advance; FSAL: k7 becomes the next k1.
+    #pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        L.y[i] = yn[i];
+        L.k1[i] = k7[i];
+    }
+    L.err_prev = (R)dmaxr(err, 1e-4);
+    L.errp_pow = (R)P::powd((double)L.err_prev, kBeta);
+    L.h = hd * fac;
+    L.c0 = ax7.cs;
+
+    if (what == BH_HIT_HORIZON || what == BH_HIT_SKY) {
+        state8(L, ptph, yh);
+    } else if (what < 0 && L.steps >= F.max_steps) {
+        what = BH_HIT_EXHAUSTED;
+        state8(L, ptph, yh);
+    }
+    if (what >= 0) {
+        write_hit(A, L, what, yh);
+        return true;
+    }
+    if (P::kMixed && rn < F.r_promote && k7[1] < R(0) && A.deferred) {
+        // Moving inwards inside the innermost photon orbit: the ray is falling
+        // in.  Hand the plunge to the binary64 kernel.
+        const unsigned long long slot = atomicAdd(&A.queue->deferred, 1ull);
+        Deferred* dd = &A.deferred[slot];
+        #pragma unroll
+        for (int i = 0; i < 6; ++i) dd->y[i] = (double)L.y[i];
+        dd->h = L.h;
+        dd->Q0 = L.Q0;
+        dd->err_prev = (float)L.err_prev;
+        dd->max_norm = L.max_norm;
+        dd->max_q = L.max_q;
+        dd->gid = L.gid;
+        dd->frame = L.frame;
+        dd->steps = L.steps;
+        dd->attempts = L.attempts;
+        dd->pad = 0;
+        return true;
+    }
+    return false;
+}
+
+template <class P, int MAXREG>
+__global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const long long total = A.resume ? (long long)*(volatile unsigned long long*)&A.queue->deferred
+                                     : A.total_rays;
+    unsigned long long* counter = A.resume ? &A.queue->resume_next : &A.queue->next;
+    Lane<P> L;
+    bool active = false, done = false;
+    long long q_next = 0;
+    int q_left = 0, q_stride = 0;
+    while (true) {
+        // A lane with ids left in its own mini-queue starts the next ray.
+        while (!active && !done && q_left > 0) {
+            if (q_next >= total) { q_left = 0; done = true; break; }
+            const long long id = q_next;
+            q_next += q_stride;
+            --q_left;
+            active = start_ray<P>(A, L, id);
+        }
+        const unsigned want = __ballot_sync(kFull, !active && !done);
+        if (want) {
+            const unsigned live = __ballot_sync(kFull, active);
+            const int n = __popc(want);
+            if (n >= A.refill || live == 0) {
+                const int leader = __ffs(want) - 1;
+                unsigned long long base = 0;
+                int stop = 0;
+                if (lane == leader) {
+                    stop = *(volatile int*)&A.queue->abort;
+                    if (!stop) base = atomicAdd(counter, (unsigned long long)n * A.rays_per_thread);
+                }
+                base = __shfl_sync(kFull, base, leader);
+                stop = __shfl_sync(kFull, stop, leader);
+                if (want & (1u << lane)) {
+                    if (stop) {
+                        done = true;
+                    } else {
+                        q_next = (long long)base + __popc(want & lt_mask);
+                        q_stride = n;
+                        q_left = A.rays_per_thread;
+                        while (!active && q_left > 0) {
+                            if (q_next >= total) { q_left = 0; break; }
+                            const long long id = q_next;
+                            q_next += q_stride;
+                            --q_left;
+                            active = start_ray<P>(A, L, id);
+                        }
+                        if (!active && q_left == 0) done = true;
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(kFull, active) == 0) {
+            if (__ballot_sync(kFull, !done) == 0) break;
+            continue;
+        }
+        if (active) {
+            if (attempt<P>(A, L)) {
+                active = false;
+                if (A.budget) atomicAdd(&A.queue->attempts, (unsigned long long)(L.attempts - L.att0));
+            }
+        }
+        if (A.budget && lane == 0) {
+            if (*(volatile unsigned long long*)&A.queue->attempts > A.budget &&
+                *(volatile int*)&A.queue->abort == 0)
+                atomicCAS(&A.queue->abort, 0, 2);
+        }
+    }
+}
+
+// Register caps (the launch parameter reg_variant picks one): binary32 lanes
+// in 128 registers (16 warps per SM) or 168; binary64 lanes in 168 (12 warps
+// per SM) or 232 (8 warps, no spills).
+constexpr int kRegMixed = 128;
+constexpr int kRegMixedWide = 168;
+constexpr int kRegFp64 = 168;
+constexpr int kRegFp64Wide = 232;
+
+template <class P, int MAXREG>
+cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, cudaStream_t s) {
+    TraceArgs A;
+    A.frames = L.frames;
+    A.frame_ray_end = L.frame_ray_end;
+    A.nframes = L.nframes;
+    A.total_rays = L.total_rays;
+    A.hits = L.hits;
+    A.queue = L.queue;
+    A.deferred = static_cast<Deferred*>(L.deferred);
+    A.resume = resume;
+    A.rays_per_thread = L.rays_per_thread < 1 ? 1 : L.rays_per_thread;
+    A.refill = L.refill < 1 ? 1 : (L.refill > 32 ? 32 : L.refill);
+    A.budget = L.budget;
+    trace_kernel<P, MAXREG><<<grid, L.block_size, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+const void* kernel_of(int precision, int variant, int resume) {
+    if (precision == BH_PRECISION_MIXED && !resume)
+        return variant ? (const void*)trace_kernel<Mixed, kRegMixedWide> : (const void*)trace_kernel<Mixed, kRegMixed>;
+    return variant ? (const void*)trace_kernel<Fp64, kRegFp64Wide> : (const void*)trace_kernel<Fp64, kRegFp64>;
+}
+
+cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, cudaStream_t s) {
+    return L.reg_variant ? launch_t<Fp64, kRegFp64Wide>(L, resume, grid, s)
+                         : launch_t<Fp64, kRegFp64>(L, resume, grid, s);
+}
+
+}  // namespace
+
+size_t deferred_record_bytes() { return sizeof(Deferred); }
+
+cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
+    if (L.precision == BH_PRECISION_MIXED) {
+        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide>(L, 0, L.grid, stream)
+                                      : launch_t<Mixed, kRegMixed>(L, 0, L.grid, stream);
+        if (e != cudaSuccess) return e;
+        if (L.resume_event) cudaEventRecord(L.resume_event, stream);
+        // The plunges, in binary64: every block checks the deferred count.
+        return launch_fp64(L, 1, L.grid_resume, stream);
+    }
+    return launch_fp64(L, 0, L.grid, stream);
+}
+
+int trace_blocks_per_sm(int precision, int block_size, int variant) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_of(precision, variant, 0), block_size, 0);
+    return n;
+}
+
+int trace_registers(int precision, int variant) {
+    cudaFuncAttributes at;
+    cudaFuncGetAttributes(&at, kernel_of(precision, variant, 0));
+    return at.numRegs;
+}
+
+}  // namespace bhg

@@ -183,8 +183,8 @@ class Renderer:
         return outs
 
     # -- launch control ----------------------------------------------------------
-    def set_launch(self, block_size=0, rays_per_thread=0, refill=0, blocks_per_sm=0) -> None:
-        p = abi.bh_launch_params(block_size, rays_per_thread, refill, blocks_per_sm)
+    def set_launch(self, block_size=0, rays_per_thread=0, refill=0, blocks_per_sm=0, reg_variant=0) -> None:
+        p = abi.bh_launch_params(block_size, rays_per_thread, refill, blocks_per_sm, reg_variant)
         self._check(self.lib.bh_gpu_set_launch(self._h, C.byref(p)))
 
     def get_launch(self) -> dict:

@@ -201,6 +201,8 @@ typedef struct bh_launch_params {
     int32_t rays_per_thread; /* rays a lane takes per queue visit, 1..4          */
     int32_t refill;          /* lanes that must be idle before a warp refills   */
     int32_t blocks_per_sm;   /* 0 = as many as fit                              */
+    int32_t reg_variant;     /* 1: tight register cap (more warps per SM),
+                                2: wide cap (fewer spills)                      */
 } bh_launch_params;
 
 typedef struct bh_ctx bh_ctx;
