@@ -37,7 +37,9 @@ struct bh_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t abort_stream = nullptr;
     std::string err;
-    bh_launch_params launch{128, 1, 32, 0, 1};
+    // Launch shapes of the FP64 [0] and mixed [1] trace kernels (measured
+    // best on the 1024^2 edge-on frame: tight registers for FP64, wide for mixed).
+    bh_launch_params launch[2] = {{128, 1, 32, 0, 1}, {128, 1, 32, 0, 2}};
     unsigned long long budget = 0;
     std::atomic<int> abort_requested{0};
     int32_t* h_one = nullptr;          // pinned 1, source of the abort copy
@@ -220,8 +222,9 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     CK(cudaMemcpyAsync(ctx->d_queue, &q, sizeof q, cudaMemcpyHostToDevice, stream));
     ctx->h2d += static_cast<long long>(n * sizeof(FrameParams) + 2 * n * sizeof(long long) + sizeof q);
 
-    const bh_launch_params& lp = ctx->launch;
     const int prec = frames[0].precision_tag;
+    const bh_launch_params& lp = ctx->launch[prec == BH_PRECISION_MIXED ? 1 : 0];
+    const bh_launch_params& lp64 = ctx->launch[0];
     int bps = lp.blocks_per_sm > 0 ? lp.blocks_per_sm : trace_blocks_per_sm(prec, lp.block_size, lp.reg_variant == 2);
     if (bps < 1) bps = 1;
     TraceLaunch tl;
@@ -239,8 +242,12 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     tl.budget = ctx->budget;
     tl.deferred = mixed ? ctx->deferred.p : nullptr;
     tl.reg_variant = (lp.reg_variant == 2) ? 1 : 0;
+    // The binary64 pass that finishes deferred mixed-precision rays runs with
+    // the FP64 launch shape.
+    tl.block_resume = lp64.block_size;
+    tl.reg_variant_resume = (lp64.reg_variant == 2) ? 1 : 0;
     {
-        int bps64 = trace_blocks_per_sm(BH_PRECISION_FP64, lp.block_size, lp.reg_variant == 2);
+        int bps64 = trace_blocks_per_sm(BH_PRECISION_FP64, lp64.block_size, lp64.reg_variant == 2);
         tl.grid_resume = ctx->sm_count * (bps64 < 1 ? 1 : bps64);
     }
     tl.resume_event = timed ? ctx->ev[3] : nullptr;
@@ -505,9 +512,16 @@ int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz
     return finish(ctx, n, stats, nullptr, true, secs);
 }
 
-int bh_gpu_set_launch(bh_ctx* ctx, const bh_launch_params* p) {
+int bh_gpu_set_launch(bh_ctx* ctx, int precision, const bh_launch_params* p) {
     if (!ctx || !p) return BH_ERR_INVALID_ARG;
-    bh_launch_params n = ctx->launch;
+    if (precision == -1) {
+        const int rc = bh_gpu_set_launch(ctx, BH_PRECISION_FP64, p);
+        return rc != BH_OK ? rc : bh_gpu_set_launch(ctx, BH_PRECISION_MIXED, p);
+    }
+    if (precision != BH_PRECISION_FP64 && precision != BH_PRECISION_MIXED)
+        return fail(ctx, BH_ERR_INVALID_ARG, "precision must be BH_PRECISION_FP64, _MIXED or -1");
+    const int slot = precision == BH_PRECISION_MIXED ? 1 : 0;
+    bh_launch_params n = ctx->launch[slot];
     if (p->block_size) {
         if (p->block_size < 32 || p->block_size > 1024 || p->block_size % 32)
             return fail(ctx, BH_ERR_INVALID_ARG, "block_size must be a multiple of 32 in [32, 1024]");
@@ -533,16 +547,53 @@ int bh_gpu_set_launch(bh_ctx* ctx, const bh_launch_params* p) {
         n.reg_variant = p->reg_variant;
     }
     // Threads x registers of one block must fit in the SM's 64 K registers.
-    const int prec_max = (n.reg_variant == 2) ? 232 : 168;
-    if (n.block_size * prec_max > 65536)
-        return fail(ctx, BH_ERR_INVALID_ARG, "block_size too large for the register cap of the binary64 kernel");
-    ctx->launch = n;
+    if (n.block_size * trace_registers(precision, n.reg_variant == 2) > 65536)
+        return fail(ctx, BH_ERR_INVALID_ARG, "block_size too large for the kernel's register count");
+    ctx->launch[slot] = n;
     return BH_OK;
 }
 
-int bh_gpu_get_launch(const bh_ctx* ctx, bh_launch_params* p) {
-    if (!ctx || !p) return BH_ERR_INVALID_ARG;
-    *p = ctx->launch;
+int bh_gpu_get_launch(const bh_ctx* ctx, int precision, bh_launch_params* p) {
+    if (!ctx || !p || (precision != BH_PRECISION_FP64 && precision != BH_PRECISION_MIXED))
+        return BH_ERR_INVALID_ARG;
+    *p = ctx->launch[precision == BH_PRECISION_MIXED ? 1 : 0];
+    return BH_OK;
+}
+
+int bh_gpu_autotune(bh_ctx* ctx, const bh_render_config* cfg, bh_launch_params* best, double* best_ms) {
+    if (!ctx || !cfg) return BH_ERR_INVALID_ARG;
+    int rc = check_cfg_header(ctx, cfg);
+    if (rc != BH_OK) return rc;
+    const int prec = cfg->precision;
+    if (prec != BH_PRECISION_FP64 && prec != BH_PRECISION_MIXED)
+        return fail(ctx, BH_ERR_INVALID_ARG, "unknown precision");
+    const int slot = prec == BH_PRECISION_MIXED ? 1 : 0;
+    const bh_launch_params keep = ctx->launch[slot];
+    std::vector<bh_xyz> px(static_cast<size_t>(std::max(cfg->width, 1)) * std::max(cfg->height, 1));
+    bh_launch_params winner = keep;
+    double winner_ms = 1e300;
+    for (int rv = 1; rv <= 2; ++rv)
+        for (int bs : {64, 128, 256, 512})
+            for (int rpt : {1, 2, 4})
+                for (int refill : {8, 16, 24, 32}) {
+                    if (bs * trace_registers(prec, rv == 2) > 65536) continue;
+                    bh_launch_params p{bs, rpt, refill, 0, rv};
+                    ctx->launch[slot] = p;
+                    bh_render_stats st;
+                    std::memset(&st, 0, sizeof st);
+                    rc = bh_gpu_render(ctx, cfg, px.data(), &st);
+                    if (rc != BH_OK) {
+                        ctx->launch[slot] = keep;
+                        return rc;
+                    }
+                    if (st.kernel_ms < winner_ms) {
+                        winner_ms = st.kernel_ms;
+                        winner = p;
+                    }
+                }
+    ctx->launch[slot] = winner;
+    if (best) *best = winner;
+    if (best_ms) *best_ms = winner_ms;
     return BH_OK;
 }
 

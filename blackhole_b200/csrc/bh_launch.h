@@ -26,6 +26,8 @@ struct TraceLaunch {
     int reg_variant;                 // 0: default register cap, 1: the wider one
     void* deferred;                  // mixed precision: total_rays deferred records
     int grid_resume;                 // blocks of the binary64 resume launch
+    int block_resume;                // its threads per block
+    int reg_variant_resume;          // its register cap (0 tight, 1 wide)
     cudaEvent_t resume_event;        // recorded between the two launches (optional)
 };
 

@@ -52,6 +52,8 @@ constexpr double D1 = -12715105075.0 / 11282082432.0, D3 = 87487479700.0 / 32700
                  D6 = -1453857185.0 / 822651844.0, D7 = 69997945.0 / 29380423.0;
 // PI controller (Gustafsson): alpha = 0.7/5, beta = 0.4/5, safety 0.9, [0.2, 5].
 constexpr double kAlpha = 0.7 / 5.0, kBeta = 0.4 / 5.0;
+// Binary32 rays closer to a pole than sin(th) = 0.01 go to binary64.
+constexpr double kPoleSin2 = 1e-4;
 
 // ---- precision policies -------------------------------------------------------
 struct Fp64 {
@@ -602,9 +604,15 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         write_hit(A, L, what, yh);
         return true;
     }
-    if (P::kMixed && rn < F.r_promote && k7[1] < R(0) && A.deferred) {
-        // Moving inwards inside the innermost photon orbit: the ray is falling
-        // in.  Hand the plunge to the binary64 kernel.
+    if (P::kMixed && A.deferred &&
+        ((rn < F.r_promote && k7[1] < R(0)) || ax7.sn2 < R(kPoleSin2))) {
+        // Two places where binary32 state cannot carry the geodesic, handed
+        // to the binary64 kernel for the rest of the ray:
+        //  - moving inwards inside the innermost photon orbit: the ray is
+        //    falling in, and Delta -> 0 cancels every digit of the
+        //    Hamiltonian's radial terms;
+        //  - within 0.01 of a pole: sin(th) carries the L_z^2 / sin^4 term,
+        //    and th = pi - 1e-5 is only resolved to 2.4e-7 in binary32.
         const unsigned long long slot = atomicAdd(&A.queue->deferred, 1ull);
         Deferred* dd = &A.deferred[slot];
         #pragma unroll
@@ -704,7 +712,7 @@ constexpr int kRegFp64 = 168;
 constexpr int kRegFp64Wide = 232;
 
 template <class P, int MAXREG>
-cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, cudaStream_t s) {
+cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s) {
     TraceArgs A;
     A.frames = L.frames;
     A.frame_ray_end = L.frame_ray_end;
@@ -717,7 +725,7 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, cudaStream_t s)
     A.rays_per_thread = L.rays_per_thread < 1 ? 1 : L.rays_per_thread;
     A.refill = L.refill < 1 ? 1 : (L.refill > 32 ? 32 : L.refill);
     A.budget = L.budget;
-    trace_kernel<P, MAXREG><<<grid, L.block_size, 0, s>>>(A);
+    trace_kernel<P, MAXREG><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
 }
 
@@ -727,9 +735,9 @@ const void* kernel_of(int precision, int variant, int resume) {
     return variant ? (const void*)trace_kernel<Fp64, kRegFp64Wide> : (const void*)trace_kernel<Fp64, kRegFp64>;
 }
 
-cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, cudaStream_t s) {
-    return L.reg_variant ? launch_t<Fp64, kRegFp64Wide>(L, resume, grid, s)
-                         : launch_t<Fp64, kRegFp64>(L, resume, grid, s);
+cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, int block, int variant, cudaStream_t s) {
+    return variant ? launch_t<Fp64, kRegFp64Wide>(L, resume, grid, block, s)
+                   : launch_t<Fp64, kRegFp64>(L, resume, grid, block, s);
 }
 
 }  // namespace
@@ -738,14 +746,14 @@ size_t deferred_record_bytes() { return sizeof(Deferred); }
 
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
     if (L.precision == BH_PRECISION_MIXED) {
-        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide>(L, 0, L.grid, stream)
-                                      : launch_t<Mixed, kRegMixed>(L, 0, L.grid, stream);
+        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide>(L, 0, L.grid, L.block_size, stream)
+                                      : launch_t<Mixed, kRegMixed>(L, 0, L.grid, L.block_size, stream);
         if (e != cudaSuccess) return e;
         if (L.resume_event) cudaEventRecord(L.resume_event, stream);
-        // The plunges, in binary64: every block checks the deferred count.
-        return launch_fp64(L, 1, L.grid_resume, stream);
+        // The deferred rays, in binary64: every block reads the deferred count.
+        return launch_fp64(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);
     }
-    return launch_fp64(L, 0, L.grid, stream);
+    return launch_fp64(L, 0, L.grid, L.block_size, L.reg_variant, stream);
 }
 
 int trace_blocks_per_sm(int precision, int block_size, int variant) {

@@ -56,8 +56,9 @@ def load_library():
             "bh_gpu_render_device": (C.c_int, [ctx_p, cfg_p, C.c_void_p, st_p, C.c_void_p]),
             "bh_gpu_trace_rays": (C.c_int, [ctx_p, cfg_p, P(abi.bh_ray_result), st_p]),
             "bh_gpu_render_batch": (C.c_int, [ctx_p, cfg_p, C.c_int, P(P(abi.bh_xyz)), st_p]),
-            "bh_gpu_set_launch": (C.c_int, [ctx_p, P(abi.bh_launch_params)]),
-            "bh_gpu_get_launch": (C.c_int, [ctx_p, P(abi.bh_launch_params)]),
+            "bh_gpu_set_launch": (C.c_int, [ctx_p, C.c_int, P(abi.bh_launch_params)]),
+            "bh_gpu_get_launch": (C.c_int, [ctx_p, C.c_int, P(abi.bh_launch_params)]),
+            "bh_gpu_autotune": (C.c_int, [ctx_p, cfg_p, P(abi.bh_launch_params), P(C.c_double)]),
             "bh_gpu_set_step_budget": (C.c_int, [ctx_p, C.c_longlong]),
             "bh_gpu_request_abort": (None, [ctx_p]),
             "bh_gpu_clear_abort": (None, [ctx_p]),
@@ -183,14 +184,24 @@ class Renderer:
         return outs
 
     # -- launch control ----------------------------------------------------------
-    def set_launch(self, block_size=0, rays_per_thread=0, refill=0, blocks_per_sm=0, reg_variant=0) -> None:
+    def set_launch(self, block_size=0, rays_per_thread=0, refill=0, blocks_per_sm=0, reg_variant=0,
+                   precision: int = -1) -> None:
+        """Launch shape of the trace kernel of `precision` (-1: both)."""
         p = abi.bh_launch_params(block_size, rays_per_thread, refill, blocks_per_sm, reg_variant)
-        self._check(self.lib.bh_gpu_set_launch(self._h, C.byref(p)))
+        self._check(self.lib.bh_gpu_set_launch(self._h, precision, C.byref(p)))
 
-    def get_launch(self) -> dict:
+    def get_launch(self, precision: int = abi.PRECISION_FP64) -> dict:
         p = abi.bh_launch_params()
-        self._check(self.lib.bh_gpu_get_launch(self._h, C.byref(p)))
+        self._check(self.lib.bh_gpu_get_launch(self._h, precision, C.byref(p)))
         return {k: getattr(p, k) for k, _ in p._fields_}
+
+    def autotune(self, cfg) -> tuple:
+        """Sweep the launch shapes on `cfg`; keeps and returns (best, ms)."""
+        c = _as_c(cfg)
+        p = abi.bh_launch_params()
+        ms = C.c_double(0.0)
+        self._check(self.lib.bh_gpu_autotune(self._h, C.byref(c), C.byref(p), C.byref(ms)))
+        return {k: getattr(p, k) for k, _ in p._fields_}, ms.value
 
     def set_step_budget(self, budget: int) -> None:
         self._check(self.lib.bh_gpu_set_step_budget(self._h, budget))

@@ -242,9 +242,18 @@ int  bh_gpu_trace_rays(bh_ctx* ctx, const bh_render_config* cfg,
 int  bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n,
                          bh_xyz* const* outs, bh_render_stats* stats);
 
-/* Launch shape used by the next calls; zero fields keep the current value. */
-int  bh_gpu_set_launch(bh_ctx* ctx, const bh_launch_params* p);
-int  bh_gpu_get_launch(const bh_ctx* ctx, bh_launch_params* p);
+/* Launch shape of the trace kernel of `precision` (BH_PRECISION_*, or -1 for
+   both) used by the next calls; zero fields keep the current value.  The
+   binary64 pass that finishes mixed-precision rays uses the FP64 shape. */
+int  bh_gpu_set_launch(bh_ctx* ctx, int precision, const bh_launch_params* p);
+int  bh_gpu_get_launch(const bh_ctx* ctx, int precision, bh_launch_params* p);
+
+/* Autotuner: render `cfg` once per launch shape of the search space (block
+   size 64..512, rays per thread 1..4, refill threshold 8..32 idle lanes,
+   both register caps), keep the shape with the shortest trace-kernel time for
+   cfg->precision, and return it in *best (and its time in *best_ms).  Extension;
+   no counterpart in the reference. */
+int  bh_gpu_autotune(bh_ctx* ctx, const bh_render_config* cfg, bh_launch_params* best, double* best_ms);
 
 /* Step budget of one launch (total step attempts over all rays; 0 = none).
    A launch that exceeds it stops taking rays and returns BH_ERR_BUDGET. */

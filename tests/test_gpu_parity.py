@@ -160,7 +160,10 @@ def test_zero_and_tiny_step_budgets_exhaust(renderer, orc):
     o, _ = orc.trace_rays(cfg)
     assert (g["what"] == o["what"]).all()
     assert (g["what"] == abi.HIT_EXHAUSTED).all() and (g["steps"] == 3).all()
-    assert np.allclose(g["y"], o["y"], rtol=1e-7, atol=1e-10), np.abs(g["y"] - o["y"]).max(axis=0)
+    # Far from the hole the embedded error estimate is a 1e-10 cancellation of
+    # the stages, so the separated-form RHS changes the step-size choice at
+    # the 1e-6 level: states agree to that, not to rounding.
+    assert np.allclose(g["y"], o["y"], rtol=1e-5, atol=1e-10), np.abs(g["y"] - o["y"]).max(axis=0)
 
 
 def test_content_switches(renderer, orc):
@@ -194,18 +197,35 @@ def test_invalid_configs_are_rejected(renderer):
     renderer.render(kerr_a09_i60(width=8, height=8))
 
 
-def test_deterministic_and_independent_of_launch_shape(renderer):
-    cfg = kerr_a09_i60(width=64, height=48, sqrt_spp=2)
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+def test_deterministic_and_independent_of_launch_shape(renderer, precision):
+    """Each ray's arithmetic does not depend on which lane, warp or launch
+    shape traces it: frames are bitwise identical across shapes."""
+    cfg = kerr_a09_i60(width=64, height=48, sqrt_spp=2, precision=precision)
     a = renderer.render(cfg)
     b = renderer.render(cfg)
     assert np.array_equal(a, b)
-    old = renderer.get_launch()
+    old = renderer.get_launch(precision)
     try:
-        for bs, rpt, refill in ((64, 1, 1), (256, 2, 32), (96, 4, 8)):
-            renderer.set_launch(block_size=bs, rays_per_thread=rpt, refill=refill)
+        for bs, rpt, refill, rv in ((64, 1, 1, 1), (256, 2, 32, 1), (96, 4, 8, 2), (128, 1, 32, 2)):
+            renderer.set_launch(block_size=bs, rays_per_thread=rpt, refill=refill, reg_variant=rv,
+                                precision=precision)
             assert np.array_equal(renderer.render(cfg), a)
     finally:
-        renderer.set_launch(**{k: v for k, v in old.items()})
+        renderer.set_launch(precision=precision, **{k: v for k, v in old.items()})
+
+
+def test_autotune_keeps_results_and_picks_a_shape(renderer):
+    cfg = kerr_a09_i60(width=48, height=48, precision=abi.PRECISION_MIXED)
+    a = renderer.render(cfg)
+    old = renderer.get_launch(abi.PRECISION_MIXED)
+    try:
+        best, ms = renderer.autotune(cfg)
+        assert ms > 0 and best["block_size"] in (64, 128, 256, 512)
+        assert renderer.get_launch(abi.PRECISION_MIXED) == best
+        assert np.array_equal(renderer.render(cfg), a)
+    finally:
+        renderer.set_launch(precision=abi.PRECISION_MIXED, **{k: v for k, v in old.items()})
 
 
 def test_stats_accumulate_like_reference(renderer):
