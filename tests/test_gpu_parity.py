@@ -200,17 +200,26 @@ def test_invalid_configs_are_rejected(renderer):
 @pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
 def test_deterministic_and_independent_of_launch_shape(renderer, precision):
     """Each ray's arithmetic does not depend on which lane, warp or launch
-    shape traces it: frames are bitwise identical across shapes."""
+    shape traces it: within one compiled kernel (register cap) frames are
+    bitwise identical across block sizes, refill thresholds and rays per
+    thread.  The two register caps are two compilations, whose mul+add
+    fusion may differ: they agree to the parity tolerance."""
     cfg = kerr_a09_i60(width=64, height=48, sqrt_spp=2, precision=precision)
-    a = renderer.render(cfg)
-    b = renderer.render(cfg)
-    assert np.array_equal(a, b)
     old = renderer.get_launch(precision)
+    tol = FP64_TOL if precision == abi.PRECISION_FP64 else MIXED_G_TOL
     try:
-        for bs, rpt, refill, rv in ((64, 1, 1, 1), (256, 2, 32, 1), (96, 4, 8, 2), (128, 1, 32, 2)):
-            renderer.set_launch(block_size=bs, rays_per_thread=rpt, refill=refill, reg_variant=rv,
-                                precision=precision)
-            assert np.array_equal(renderer.render(cfg), a)
+        frames = {}
+        for rv in (1, 2):
+            renderer.set_launch(block_size=128, rays_per_thread=1, refill=32, reg_variant=rv, precision=precision)
+            a = renderer.render(cfg)
+            assert np.array_equal(a, renderer.render(cfg))
+            for bs, rpt, refill in ((64, 1, 1), (256, 2, 32), (96, 4, 8)):
+                renderer.set_launch(block_size=bs, rays_per_thread=rpt, refill=refill, precision=precision)
+                assert np.array_equal(renderer.render(cfg), a), (rv, bs, rpt, refill)
+            frames[rv] = a
+        lit = frames[1][..., 1] > 0
+        rel = np.abs(frames[1][..., 1][lit] - frames[2][..., 1][lit]) / frames[1][..., 1][lit]
+        assert q(rel, 0.99) <= tol
     finally:
         renderer.set_launch(precision=precision, **{k: v for k, v in old.items()})
 
