@@ -136,6 +136,44 @@ class bh_launch_params(C.Structure):
     ]
 
 
+class bh_trace_record(C.Structure):
+    _fields_ = [
+        ("y", C.c_double * 8), ("max_norm", C.c_double), ("max_q", C.c_double),
+        ("what", C.c_int32), ("steps", C.c_int32), ("attempts", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
+NOALLOC_MAX_RAYS = 65536
+
+
+def trace_record_dtype():
+    import numpy as np
+
+    return np.dtype({
+        "names": ["y", "max_norm", "max_q", "what", "steps", "attempts"],
+        "formats": [(np.float64, 8), np.float64, np.float64, np.int32, np.int32, np.int32],
+        "offsets": [0, 64, 72, 80, 84, 88],
+        "itemsize": C.sizeof(bh_trace_record),
+    })
+
+
+def work_order(width: int, height: int, sqrt_spp: int):
+    """Row-major sample index (pixel row-major, then sample) of each ray id in
+    the library's work order (bands of four rows, column by column)."""
+    import numpy as np
+
+    s = max(1, sqrt_spp)
+    ss = s * s
+    p = np.arange(width * height, dtype=np.int64)
+    band = p // (4 * width)
+    rel = p - band * 4 * width
+    bh = np.minimum(4, height - 4 * band)
+    x = rel // bh
+    y = 4 * band + rel % bh
+    pix = y * width + x
+    return (pix[:, None] * ss + np.arange(ss)[None, :]).reshape(-1)
+
+
 # numpy dtype of bh_ray_result, for zero-copy views of result arrays.
 def ray_result_dtype():
     import numpy as np

@@ -33,6 +33,7 @@ struct TraceLaunch {
 
 // Bytes of one deferred-ray record.
 size_t deferred_record_bytes();
+constexpr size_t kDeferredRecordBytes = 96;   // checked against the record in bh_trace.cu
 
 // Persistent trace kernel over all rays of all frames.
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream);

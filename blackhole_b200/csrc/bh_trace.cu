@@ -269,6 +269,7 @@ struct Deferred {
     float err_prev, max_norm, max_q;
     int gid, frame, steps, attempts, pad;
 };
+static_assert(sizeof(Deferred) == kDeferredRecordBytes, "kDeferredRecordBytes is stale");
 
 struct TraceArgs {
     const FrameParams* frames;

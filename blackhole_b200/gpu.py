@@ -65,6 +65,7 @@ def load_library():
             "bh_star_catalogue": (C.c_int, [C.c_int, C.c_uint64, C.c_int, P(C.c_double)]),
             "bh_blackbody_table": (C.c_int, [P(C.c_double)]),
             "bh_gpu_fma_peak": (C.c_int, [C.c_int, C.c_int, P(C.c_double)]),
+            "bh_gpu_trace_noalloc": (C.c_int, [C.c_int, cfg_p, C.c_void_p, C.c_void_p]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(lib, name)

@@ -264,6 +264,48 @@ int  bh_gpu_set_step_budget(bh_ctx* ctx, long long budget);
 void bh_gpu_request_abort(bh_ctx* ctx);
 void bh_gpu_clear_abort(bh_ctx* ctx);
 
+/* One ray's trace result, without shading: final state (t, r, th, phi, p_t,
+   p_r, p_th, p_phi), the worst relative null norm and Carter drift along the
+   ray, its termination class (BH_HIT_*), accepted steps and step attempts. */
+typedef struct bh_trace_record {
+    double y[8];
+    double max_norm;
+    double max_q;
+    int32_t what;
+    int32_t steps;
+    int32_t attempts;
+    int32_t reserved;
+} bh_trace_record;
+
+/* Largest ray count (width * height * sqrt_spp^2) bh_gpu_trace_noalloc takes. */
+#define BH_NOALLOC_MAX_RAYS 65536
+
+/* Trace the rays of `cfg` into the caller's device buffer d_out (n_rays
+   bh_trace_record) on `stream` (a cudaStream_t; NULL = the legacy default
+   stream), WITHOUT allocating: for callers that cannot call cudaMalloc -
+   hosts whose GPU memory belongs to their own allocator or fixed budget
+   (engines, frameworks with a caching allocator, plug-in hosts that forbid
+   device allocation in the render callback), and real-time loops that cannot
+   afford the implicit device synchronisation cudaMalloc/cudaFree may cause.
+   It allocates no device memory, and on success no host memory either.
+   The kernel's scratch (work-queue counters, frame constants, and for
+   BH_PRECISION_MIXED the list of rays handed to binary64) lives in one
+   statically allocated 6.3 MiB device array of this library, so a call
+   takes at most BH_NOALLOC_MAX_RAYS rays and returns BH_ERR_INVALID_ARG
+   above that.  Every GPU that loads the library holds the array until exit.
+   The first call on a device looks the array's device address up (do it
+   before any stream capture); every call clears the counters it needs at
+   zero, and all calls share the one array, so calls whose work overlaps on
+   the GPU (other streams, other host threads) race - serialise them.
+   Stars, disc temperature and pixels are not computed (no shading): the
+   records equal the trace part of bh_gpu_trace_rays for the same config and
+   default launch shape.  Records are in work order: ray id = p * S^2 + k for
+   sample k = sy * S + sx of pixel p, with pixels numbered in bands of four
+   rows, column by column inside a band (band b = p / (4 W) covers rows
+   4b .. 4b + h - 1, h = min(4, H - 4b); x = (p - 4Wb) / h, y = 4b + (p - 4Wb) % h).
+   Returns once the work is enqueued.  No counterpart in the reference. */
+int  bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_trace_record* d_out, void* stream);
+
 /* Measured FMA throughput of `device` in TFLOP/s (2 FLOP per FMA) for
    BH_PRECISION_FP64 (binary64) or BH_PRECISION_MIXED (binary32): the ALU
    roofline of the trace kernel.  Extension; no counterpart in the reference. */

@@ -48,6 +48,7 @@ STRUCTS = {
     "bh_neutron_star": abi.bh_neutron_star,
     "bh_launch_params": abi.bh_launch_params,
     "bh_xyz": abi.bh_xyz,
+    "bh_trace_record": abi.bh_trace_record,
 }
 
 
