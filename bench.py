@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--size", type=int, default=1024, help="frame side (default 1024)")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--once", action="store_true",
+                   help="render the frame once in mixed precision and once in FP64 and exit (for ncu captures)")
     return p.parse_args()
 
 
@@ -417,9 +419,25 @@ def reference_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def once(args):
+    """One render per precision: the launch list of a profiler capture is
+    trace (mixed), trace (binary64 resume), shade, 2 x reduce, then trace
+    (FP64), shade, 2 x reduce."""
+    from blackhole_b200 import Renderer, RenderStats, abi
+
+    with Renderer(0) as r:
+        for prec in (abi.PRECISION_MIXED, abi.PRECISION_FP64):
+            st = RenderStats()
+            r.render(frame_config(args.size, 0, 1, prec), st)
+            print(json.dumps({"precision": prec, "kernel_ms": st.kernel_ms, "steps": st.steps,
+                              "attempts": st.attempts, "rays": st.rays}), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.once:
+        once(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

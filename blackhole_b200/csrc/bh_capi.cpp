@@ -453,7 +453,9 @@ int bh_gpu_render_device(bh_ctx* ctx, const bh_render_config* cfg, bh_xyz* d_pix
     std::vector<FrameParams> frames;
     int rc = prepare_frames(ctx, cfg, 1, frames);
     if (rc != BH_OK) return rc;
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    // NULL is the legacy default stream, ordered with the caller's other
+    // default-stream work (the context's own stream is non-blocking).
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
     rc = enqueue(ctx, frames, d_pixels, nullptr, s, stats != nullptr);
     if (rc != BH_OK || !stats) return rc;
     CK(cudaStreamSynchronize(s));

@@ -145,7 +145,8 @@ struct Lane {
     R k1[6];                 // FSAL stage
     R E, Lz, aR, a2R, aE, aLz, a2E2, Lz2;
     R rp_hi, rp_lo, rm_hi, rm_lo;   // r_+ and r_- as exact two-term sums
-    R c0;                    // cos(th) at y, for the disc-plane test
+    R c0;                    // cos(th) at y (disc-plane test, stage angles)
+    R sn0;                   // sin(th) at y as the metric clamps it (stage angles)
     double h;
     R err_prev, errp_pow;    // PI-controller memory and pow(err_prev, beta)
     double Q0;
@@ -160,32 +161,55 @@ struct Lane {
 
 template <class P>
 struct Aux {
-    typename P::R cs, sn2, cs2, D;
+    typename P::R sn, cs, sn2, cs2, D;
 };
+
+// sin and cos of th0 + d from those of th0, |d| <= kMaxShift: angle addition
+// with Taylor series of sin d and cos d (to d^7 / d^6 in binary32, d^13 /
+// d^14 in binary64: truncation below the format's rounding for |d| <= 1/4).
+constexpr double kMaxShift = 0.25;
+
+__device__ __forceinline__ void shift_sincos(float s0, float c0, float d, float* s, float* c) {
+    const float d2 = d * d;
+    const float sd = d * (1.f - d2 * (1.f / 6.f) * (1.f - d2 * (1.f / 20.f) * (1.f - d2 * (1.f / 42.f))));
+    const float cd = 1.f - d2 * 0.5f * (1.f - d2 * (1.f / 12.f) * (1.f - d2 * (1.f / 30.f)));
+    *s = s0 * cd + c0 * sd;
+    *c = c0 * cd - s0 * sd;
+}
+__device__ __forceinline__ void shift_sincos(double s0, double c0, double d, double* s, double* c) {
+    const double d2 = d * d;
+    const double sd = d * (1.0 - d2 / 6.0 * (1.0 - d2 / 20.0 * (1.0 - d2 / 42.0 * (1.0 - d2 / 72.0 *
+                      (1.0 - d2 / 110.0 * (1.0 - d2 / 156.0))))));
+    const double cd = 1.0 - d2 * 0.5 * (1.0 - d2 / 12.0 * (1.0 - d2 / 30.0 * (1.0 - d2 / 56.0 *
+                      (1.0 - d2 / 90.0 * (1.0 - d2 / 132.0 * (1.0 - d2 / 182.0))))));
+    *s = s0 * cd + c0 * sd;
+    *c = c0 * cd - s0 * sd;
+}
 
 // Hamilton's equations for H = 1/2 g^{mu nu} p_mu p_nu (geodesic.h:50-71),
 // with the Kerr inverse metric in Carter's separated form
 //   2 Sigma H = Delta p_r^2 + p_th^2 + (L_z - a E sin^2)^2 / sin^2
 //               - ((r^2 + a^2) E - a L_z)^2 / Delta,
 // E = -p_t and L_z = p_phi constant (their derivatives vanish exactly).  The
-// same function of (r, th, p) as the reference's quotient-rule form; three
-// reciprocals instead of fifteen divisions.  H = 0 is not imposed (B is the
-// full bracket).  Delta = (r - r_+)(r - r_-) with each factor formed against
-// a two-term r_+-, so the factor that vanishes at the horizon is exact.
+// same function of (r, th, p) as the reference's quotient-rule form, with one
+// reciprocal (of Sigma Delta sin^2) instead of fifteen divisions.  H = 0 is
+// not imposed (B is the full bracket).  Delta = (r - r_+)(r - r_-) with each
+// factor formed against a two-term r_+-, so the factor that vanishes at the
+// horizon is exact.  sn, cs: sin and cos of th.
 template <class P>
-__device__ __forceinline__ void rhs(const Lane<P>& L, typename P::R r, typename P::R th,
-                                    typename P::R pr, typename P::R pth, typename P::R* d,
-                                    Aux<P>* aux) {
+__device__ __forceinline__ void rhs_sc(const Lane<P>& L, typename P::R r, typename P::R sn,
+                                       typename P::R cs, typename P::R pr, typename P::R pth,
+                                       typename P::R* d, Aux<P>* aux) {
     using R = typename P::R;
-    R sn, cs;
-    P::sc(th, &sn, &cs);
     if (fabs(sn) < R(1e-9)) sn = (sn < R(0)) ? R(-1e-9) : R(1e-9);   // kerr.h:51
     const R sn2 = sn * sn, cs2 = cs * cs;
     const R r2 = r * r;
     const R S = r2 + L.a2R * cs2;
     const R D = L.factored ? ((r - L.rp_hi) - L.rp_lo) * ((r - L.rm_hi) - L.rm_lo)
                            : (r2 - R(2) * r + L.a2R);
-    const R iS = P::rcp(S), iD = P::rcp(D), isn2 = P::rcp(sn2);
+    const R SD = S * D;
+    const R inv = P::rcp(SD * sn2);
+    const R iS = inv * D * sn2, iD = inv * S * sn2, isn2 = inv * SD;
     const R r2a2 = r2 + L.a2R;
     const R K = r2a2 * L.E - L.aLz;
     const R Lp = L.Lz - L.aE * sn2;
@@ -199,11 +223,36 @@ __device__ __forceinline__ void rhs(const Lane<P>& L, typename P::R r, typename 
     d[4] = R(-0.5) * iS * (Dr * pr * pr - R(4) * r * L.E * KiD + Dr * KiD * KiD - R(2) * r * B * iS);
     d[5] = -sn * cs * iS * (L.a2E2 - L.Lz2 * isn2 * isn2 + L.a2R * B * iS);
     if (aux) {
+        aux->sn = sn;
         aux->cs = cs;
         aux->sn2 = sn2;
         aux->cs2 = cs2;
         aux->D = D;
     }
+}
+
+// The RHS at a fresh angle (full sincos).
+template <class P>
+__device__ __forceinline__ void rhs(const Lane<P>& L, typename P::R r, typename P::R th,
+                                    typename P::R pr, typename P::R pth, typename P::R* d,
+                                    Aux<P>* aux) {
+    typename P::R sn, cs;
+    P::sc(th, &sn, &cs);
+    rhs_sc<P>(L, r, sn, cs, pr, pth, d, aux);
+}
+
+// The RHS at a stage angle th, from the sin/cos of the step's base angle
+// L.y[2] by angle addition (full sincos when the stage moved th by more
+// than kMaxShift).
+template <class P>
+__device__ __forceinline__ void rhs_stage(const Lane<P>& L, typename P::R r, typename P::R th,
+                                          typename P::R pr, typename P::R pth, typename P::R* d) {
+    using R = typename P::R;
+    const R dth = th - L.y[2];
+    R sn, cs;
+    if (fabs(dth) <= R(kMaxShift)) shift_sincos(L.sn0, L.c0, dth, &sn, &cs);
+    else P::sc(th, &sn, &cs);
+    rhs_sc<P>(L, r, sn, cs, pr, pth, d, nullptr);
 }
 
 // Dense-output polynomial of one component (geodesic.h:109-121, 176-185).
@@ -404,39 +453,45 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         Aux<P> ax;
         rhs<P>(L, L.y[1], L.y[2], L.y[4], L.y[5], L.k1, &ax);
         L.c0 = ax.cs;
+        L.sn0 = ax.sn;
         L.have_k1 = 1;
     }
     const R h = (R)L.h;
     R t[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], yn[6];
     #pragma unroll
     for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * R(A21) * L.k1[i];
-    rhs<P>(L, t[1], t[2], t[4], t[5], k2, nullptr);
+    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k2);
     #pragma unroll
     for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * (R(A31) * L.k1[i] + R(A32) * k2[i]);
-    rhs<P>(L, t[1], t[2], t[4], t[5], k3, nullptr);
+    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k3);
     #pragma unroll
     for (int i = 0; i < 6; ++i)
         t[i] = L.y[i] + h * (R(A41) * L.k1[i] + R(A42) * k2[i] + R(A43) * k3[i]);
-    rhs<P>(L, t[1], t[2], t[4], t[5], k4, nullptr);
+    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k4);
     #pragma unroll
     for (int i = 0; i < 6; ++i)
         t[i] = L.y[i] + h * (R(A51) * L.k1[i] + R(A52) * k2[i] + R(A53) * k3[i] + R(A54) * k4[i]);
-    rhs<P>(L, t[1], t[2], t[4], t[5], k5, nullptr);
+    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k5);
     #pragma unroll
     for (int i = 0; i < 6; ++i)
         t[i] = L.y[i] + h * (R(A61) * L.k1[i] + R(A62) * k2[i] + R(A63) * k3[i] +
                              R(A64) * k4[i] + R(A65) * k5[i]);
-    rhs<P>(L, t[1], t[2], t[4], t[5], k6, nullptr);
+    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k6);
     #pragma unroll
     for (int i = 0; i < 6; ++i)
         yn[i] = L.y[i] + h * (R(B1) * L.k1[i] + R(B3) * k3[i] + R(B4) * k4[i] + R(B5) * k5[i] +
                               R(B6) * k6[i]);
+    // The last stage is the next step's first (FSAL) and its angle the next
+    // base angle: full sincos, so angle-addition errors never chain.
     Aux<P> ax7;
     rhs<P>(L, yn[1], yn[2], yn[4], yn[5], k7, &ax7);
 
     // RMS error over the eight components (geodesic.h:157-166): the p_t and
-    // p_phi terms are exactly zero.  Squares summed in binary64.
+    // p_phi terms are exactly zero.  binary64: squares summed in binary64;
+    // mixed: scaled errors and their squares in binary32, the norm and the
+    // accept/reject test in binary64.
     double err2 = 0.0;
+    float err2f = 0.f;
     #pragma unroll
     for (int i = 0; i < 6; ++i) {
         const R e = h * (R(E1) * L.k1[i] + R(E3) * k3[i] + R(E4) * k4[i] + R(E5) * k5[i] +
@@ -444,13 +499,14 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         if (P::kMixed) {
             const float sc = (float)F.atol + (float)F.rtol * fmaxf(fabsf((float)L.y[i]), fabsf((float)yn[i]));
             const float q = (float)e * Mixed::rcp(sc);
-            err2 += (double)q * (double)q;
+            err2f += q * q;
         } else {
             const double sc = F.atol + F.rtol * dmaxr(fabs((double)L.y[i]), fabs((double)yn[i]));
             const double q = (double)e / sc;
             err2 += q * q;
         }
     }
+    if (P::kMixed) err2 = (double)err2f;
     double err = sqrt(err2 / 8.0);
     if (L.bad_sc || !isfinite(err)) err = 1e10;
     ++L.attempts;
@@ -594,6 +650,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     L.errp_pow = (R)P::powd((double)L.err_prev, kBeta);
     L.h = hd * fac;
     L.c0 = ax7.cs;
+    L.sn0 = ax7.sn;
 
     if (what == BH_HIT_HORIZON || what == BH_HIT_SKY) {
         state8(L, ptph, yh);

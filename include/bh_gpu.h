@@ -225,7 +225,7 @@ int  bh_gpu_render(bh_ctx* ctx, const bh_render_config* cfg,
                    bh_xyz* out_pixels, bh_render_stats* stats);
 
 /* The same frame, written into a device buffer of W*H bh_xyz on `stream`
-   (a cudaStream_t, or NULL for the context's stream).  Returns once the work
+   (a cudaStream_t, or NULL for the legacy default stream).  Returns once the work
    is enqueued when stats == NULL; with stats it synchronises. */
 int  bh_gpu_render_device(bh_ctx* ctx, const bh_render_config* cfg,
                           bh_xyz* d_pixels, bh_render_stats* stats, void* stream);

@@ -206,7 +206,9 @@ def test_deterministic_and_independent_of_launch_shape(renderer, precision):
     fusion may differ: they agree to the parity tolerance."""
     cfg = kerr_a09_i60(width=64, height=48, sqrt_spp=2, precision=precision)
     old = renderer.get_launch(precision)
-    tol = FP64_TOL if precision == abi.PRECISION_FP64 else MIXED_G_TOL
+    # pixel luminance: the blackbody Y of g T moves like g^3..g^5 in the
+    # visible tail, so the mixed path's 1e-3 in g is up to ~1e-2 in Y
+    tol = FP64_TOL if precision == abi.PRECISION_FP64 else 10 * MIXED_G_TOL
     try:
         frames = {}
         for rv in (1, 2):
