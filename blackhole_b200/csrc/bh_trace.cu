@@ -87,7 +87,9 @@ __device__ __forceinline__ double xs(double a, double b) { return __dsub_rn(a, b
 // Initial photon state of frame-local ray `local_id` (render.cpp:440-451,
 // scene.h:356-384, geodesic.h:215-231) and its Carter constant
 // (kerr.h:342-348, with the camera's sin^2/cos^2 precomputed on the host).
-__device__ void ray_setup(const FrameParams& F, long long local_id, double y[8], double* Q0) {
+// Out of line: it runs once per ray, and inlined it would push the step loop
+// apart in the instruction cache.
+__device__ __noinline__ void ray_setup(const FrameParams& F, long long local_id, double y[8], double* Q0) {
     const int S = F.S;
     const long long pixel = local_id / (S * S);
     const int k = (int)(local_id - pixel * (S * S));
@@ -177,11 +179,16 @@ __device__ __forceinline__ void shift_sincos(float s0, float c0, float d, float*
     *c = c0 * cd - s0 * sd;
 }
 __device__ __forceinline__ void shift_sincos(double s0, double c0, double d, double* s, double* c) {
+    // reciprocals as constants: a division by 6.0 is a real division
+    constexpr double i6 = 1.0 / 6.0, i20 = 1.0 / 20.0, i42 = 1.0 / 42.0, i72 = 1.0 / 72.0;
+    constexpr double i110 = 1.0 / 110.0, i156 = 1.0 / 156.0;
+    constexpr double i12 = 1.0 / 12.0, i30 = 1.0 / 30.0, i56 = 1.0 / 56.0, i90 = 1.0 / 90.0;
+    constexpr double i132 = 1.0 / 132.0, i182 = 1.0 / 182.0;
     const double d2 = d * d;
-    const double sd = d * (1.0 - d2 / 6.0 * (1.0 - d2 / 20.0 * (1.0 - d2 / 42.0 * (1.0 - d2 / 72.0 *
-                      (1.0 - d2 / 110.0 * (1.0 - d2 / 156.0))))));
-    const double cd = 1.0 - d2 * 0.5 * (1.0 - d2 / 12.0 * (1.0 - d2 / 30.0 * (1.0 - d2 / 56.0 *
-                      (1.0 - d2 / 90.0 * (1.0 - d2 / 132.0 * (1.0 - d2 / 182.0))))));
+    const double sd = d * (1.0 - d2 * i6 * (1.0 - d2 * i20 * (1.0 - d2 * i42 * (1.0 - d2 * i72 *
+                      (1.0 - d2 * i110 * (1.0 - d2 * i156))))));
+    const double cd = 1.0 - d2 * 0.5 * (1.0 - d2 * i12 * (1.0 - d2 * i30 * (1.0 - d2 * i56 *
+                      (1.0 - d2 * i90 * (1.0 - d2 * i132 * (1.0 - d2 * i182))))));
     *s = s0 * cd + c0 * sd;
     *c = c0 * cd - s0 * sd;
 }
@@ -531,29 +538,6 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     ++L.steps;
     const double rn = (double)yn[1];
     const double pt = -(double)L.E, pph = (double)L.Lz;
-    {
-        // Invariant diagnostics at y_new (render.cpp:139-145) in binary64.
-        // The five terms of g^{ab} p_a p_b (kerr.h:301-321) are all scaled by
-        // Sigma Delta sin^2 > 0 and Carter's Q by sin^2, which leaves both
-        // ratios unchanged; a division only when a maximum grows.
-        const double sn2 = (double)ax7.sn2, cs2 = (double)ax7.cs2, Del = (double)ax7.D;
-        const double pr = (double)yn[4], pth = (double)yn[5];
-        const double a2 = F.a2;
-        const double rpa = rn * rn + a2;
-        const double Ak = rpa * rpa - a2 * Del * sn2;
-        const double T1 = -Ak * pt * pt * sn2;
-        const double T2 = -4.0 * F.a * rn * pt * pph * sn2;
-        const double T3 = Del * Del * sn2 * pr * pr;
-        const double T4 = Del * sn2 * pth * pth;
-        const double T5 = (Del - a2 * sn2) * pph * pph;
-        const double nrm = fabs(T1 + T2 + T3 + T4 + T5);
-        const double scl = fabs(T1) + fabs(T2) + fabs(T3) + fabs(T4) + fabs(T5);
-        if (nrm > (double)L.max_norm * scl) L.max_norm = (float)((scl > 0.0) ? nrm / scl : nrm);
-        const double Qs = pth * pth * sn2 + cs2 * (a2 * (0.0 - pt * pt) * sn2 + pph * pph);
-        const double dev = fabs(Qs - L.Q0 * sn2) * (double)L.inv_Q0;
-        if (dev > (double)L.max_q * sn2) L.max_q = (float)(dev / sn2);
-    }
-
     const double hd = L.h;
     const double ptph[2] = {pt, pph};
     int what = -1;
@@ -651,6 +635,30 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     L.h = hd * fac;
     L.c0 = ax7.cs;
     L.sn0 = ax7.sn;
+
+    {
+        // Invariant diagnostics at the new state (render.cpp:139-145), in
+        // binary64, after the events so the stage values are no longer live.
+        // The five terms of g^{ab} p_a p_b (kerr.h:301-321) are all scaled by
+        // Sigma Delta sin^2 > 0 and Carter's Q by sin^2, which leaves both
+        // ratios unchanged; a division only when a maximum grows.
+        const double sn2 = (double)ax7.sn2, cs2 = (double)ax7.cs2, Del = (double)ax7.D;
+        const double pr = (double)L.y[4], pth = (double)L.y[5];
+        const double a2 = F.a2;
+        const double rpa = rn * rn + a2;
+        const double Ak = rpa * rpa - a2 * Del * sn2;
+        const double T1 = -Ak * pt * pt * sn2;
+        const double T2 = -4.0 * F.a * rn * pt * pph * sn2;
+        const double T3 = Del * Del * sn2 * pr * pr;
+        const double T4 = Del * sn2 * pth * pth;
+        const double T5 = (Del - a2 * sn2) * pph * pph;
+        const double nrm = fabs(T1 + T2 + T3 + T4 + T5);
+        const double scl = fabs(T1) + fabs(T2) + fabs(T3) + fabs(T4) + fabs(T5);
+        if (nrm > (double)L.max_norm * scl) L.max_norm = (float)((scl > 0.0) ? nrm / scl : nrm);
+        const double Qs = pth * pth * sn2 + cs2 * (a2 * (0.0 - pt * pt) * sn2 + pph * pph);
+        const double dev = fabs(Qs - L.Q0 * sn2) * (double)L.inv_Q0;
+        if (dev > (double)L.max_q * sn2) L.max_q = (float)(dev / sn2);
+    }
 
     if (what == BH_HIT_HORIZON || what == BH_HIT_SKY) {
         state8(L, ptph, yh);
