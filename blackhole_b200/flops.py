@@ -1,42 +1,47 @@
 """Algorithmic floating-point work of the trace kernel, counted from its source.
 
 Unit of work: one accepted DP5(4) step of one ray (rejected attempts, ray
-set-up and event bisection are overhead).  The counts below are the add, sub
-and mul operations of the expressions in blackhole_b200/csrc/bh_kernels.cu
-(``rhs``, the stage combinations and the error norm of ``attempt``, and the
-invariant diagnostics of an accepted step), each counted once per evaluation
-with loop-invariant sub-expressions counted once; a fused multiply-add counts
-as 2, the same convention as the FMA peak (2 FLOP per FMA).  Divisions,
-reciprocals, square roots, sin/cos and pow are listed separately ("special")
-and not included in the FLOP figure.
+set-up and event location are overhead).  The counts are the add, sub and mul
+operations of the expressions in blackhole_b200/csrc/bh_trace.cu, each counted
+once per evaluation, loop-invariant sub-expressions once; a fused
+multiply-add counts 2, the convention of the FMA peak (2 FLOP per FMA).
+Reciprocals, divisions, square roots, sin/cos and pow are listed separately
+("special") and not counted.
 
-  rhs (per call):        55 real ops + 6 binary64 ops (Sigma, Delta)
-                         + 1 sincos + 3 reciprocals
-  per attempt:           6 rhs = 330 real + 36 f64
-                         stage combinations: 13 + 30 + 42 + 54 + 66 + 66 = 271 real
-                         error estimate: 6 x 12 = 72 real; norm: 6 x 4 + 1 = 25 f64,
-                         6 divisions, 1 sqrt, 1 pow
-  per accepted step:     diagnostics 43 f64, 2 divisions
+  rhs_sc (per call)        S, D (two-term factors), S*D, S*D*sin^2, iS, iD,
+                           1/sin^2 from one reciprocal, K, L', B and the six
+                           derivatives: 62 ops + 1 reciprocal
+  shift_sincos (stages 2-6) angle addition with Taylor series of sin/cos of the
+                           stage increment: 25 ops in binary32, 36 in binary64
+  stage combinations       13 + 30 + 42 + 54 + 66 + 66 = 271 ops
+  error estimate           per component 12 (stage combination) + 2 (scale)
+                           + 1 (scaled error) + 2 (square, sum) = 17, x 6 = 102;
+                           the binary64 path divides instead of multiplying by a
+                           reciprocal: 16 ops + 1 division per component
+  step control (binary64)  hmax 3, error norm 1, h update 1: 5 ops
+  diagnostics (binary64)   null-norm terms and Carter's Q: 43 ops per accepted step
 
-"real" is binary32 in the mixed path and binary64 in the FP64 path.
+Stage 7 (the FSAL stage, the next step's base angle) and the first stage of a
+ray take a full sincos.
 """
 
-RHS_REAL = 55
-RHS_F64 = 6
-STAGES_REAL = 13 + 30 + 42 + 54 + 66 + 66
-ERROR_REAL = 6 * 12
-ERROR_F64 = 6 * 4 + 1
+RHS = 62
+SHIFT = {"mixed": 25, "fp64": 36}
+STAGES = 13 + 30 + 42 + 54 + 66 + 66
+ERROR = {"mixed": 6 * 17, "fp64": 6 * 16}
+CONTROL_F64 = 5
 DIAG_F64 = 43
 
-PER_ATTEMPT_REAL = 6 * RHS_REAL + STAGES_REAL + ERROR_REAL          # 673
-PER_ATTEMPT_F64 = 6 * RHS_F64 + ERROR_F64                           # 61
 
-# FLOPs per accepted step charged against the ALU peak of the path's main pipe.
-FLOPS_PER_STEP = {
-    # mixed: binary32 work against the FP32 peak; binary64 islands listed apart
-    "mixed": {"alu_flop": PER_ATTEMPT_REAL, "f64_flop": PER_ATTEMPT_F64 + DIAG_F64,
-              "special": {"sincos": 6, "rcp": 18, "div_f64": 8, "sqrt_f64": 1, "pow_f32": 1}},
-    # fp64: everything binary64 against the FP64 peak
-    "fp64": {"alu_flop": PER_ATTEMPT_REAL + PER_ATTEMPT_F64 + DIAG_F64, "f64_flop": 0,
-             "special": {"sincos": 6, "div_f64": 26, "sqrt_f64": 1, "pow_f64": 1}},
-}
+def per_step(path: str) -> dict:
+    alu = 6 * RHS + 5 * SHIFT[path] + STAGES + ERROR[path]
+    if path == "mixed":
+        return {"alu_flop": alu, "f64_flop": CONTROL_F64 + DIAG_F64,
+                "special": {"sincos_f32": 1, "rcp_f32": 6 + 6, "pow_f32": 2, "sqrt_f64": 1}}
+    return {"alu_flop": alu + CONTROL_F64 + DIAG_F64, "f64_flop": 0,
+            "special": {"sincos_f64": 1, "div_f64": 6 + 6, "pow_f64": 2, "sqrt_f64": 1}}
+
+
+# FLOPs per accepted step charged against the ALU peak of each path's main pipe:
+# mixed 870 binary32 (+ 48 binary64 islands), fp64 967 binary64.
+FLOPS_PER_STEP = {"mixed": per_step("mixed"), "fp64": per_step("fp64")}
