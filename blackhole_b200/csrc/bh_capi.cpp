@@ -60,6 +60,17 @@ struct bh_ctx {
     QueueState* d_queue = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     long long h2d = 0, d2h = 0;          // bytes copied by the current call
+
+    // Pinned staging of the per-launch constants, and the event after which
+    // the last launch no longer reads it.
+    unsigned char* stage = nullptr;
+    size_t stage_cap = 0;
+    cudaEvent_t stage_free = nullptr;
+
+    // The captured CUDA graph of the last batch shape (bh_gpu_render_batch),
+    // keyed by the launch descriptors it was captured from.
+    cudaGraphExec_t batch_exec = nullptr;
+    std::vector<unsigned char> batch_key;
 };
 
 namespace {
@@ -183,22 +194,33 @@ void stats_add(bh_render_stats* s, const FrameStats& f) {
     s->total_flux += f.total_flux;
 }
 
-// Enqueue the whole pipeline for `frames` on `stream`.  Pixels go to
-// `d_pixels` (frame-major, row-major), per-sample results to `d_rays` when
-// given (single frame only).
-int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_ray_result* d_rays,
-            cudaStream_t stream, bool timed) {
+// One launch of the pipeline, planned on the host.
+struct Plan {
+    int n = 0;
+    long long rays = 0, pix = 0;
+    bool mixed = false;
+    TraceLaunch tl;
+    ShadeLaunch sl;
+    ReduceLaunch rl;
+    size_t stage_bytes = 0;
+};
+
+// Host half of a launch: size the device buffers (all allocation happens
+// here) and write the frame constants, cumulative ends and the queue's
+// initial state into the context's pinned staging buffer.
+int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_ray_result* d_rays,
+                bool timed, Plan& p) {
     const int n = static_cast<int>(frames.size());
-    std::vector<long long> ray_end(n), pix_end(n);
+    p.n = n;
     long long rays = 0, pix = 0;
     for (int i = 0; i < n; ++i) {
         frames[i].ray_begin = rays;
         frames[i].pixel_begin = pix;
         rays += frames[i].n_rays;
         pix += static_cast<long long>(frames[i].width) * frames[i].height;
-        ray_end[i] = rays;
-        pix_end[i] = pix;
     }
+    p.rays = rays;
+    p.pix = pix;
     int rc;
     if ((rc = ensure(ctx, ctx->hits, static_cast<size_t>(rays) * sizeof(HitRecord))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->lum, static_cast<size_t>(pix) * sizeof(double))) != BH_OK) return rc;
@@ -208,26 +230,41 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     if ((rc = ensure(ctx, ctx->partials, static_cast<size_t>(n) * kReduceBlocks * sizeof(FrameStats))) != BH_OK)
         return rc;
     if ((rc = ensure(ctx, ctx->fstats, n * sizeof(FrameStats))) != BH_OK) return rc;
-    const bool mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
-    if (mixed && (rc = ensure(ctx, ctx->deferred, static_cast<size_t>(rays) * deferred_record_bytes())) != BH_OK)
+    p.mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
+    if (p.mixed && (rc = ensure(ctx, ctx->deferred, static_cast<size_t>(rays) * deferred_record_bytes())) != BH_OK)
         return rc;
 
-    CK(cudaMemcpyAsync(ctx->frames.p, frames.data(), n * sizeof(FrameParams), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(ctx->ray_end.p, ray_end.data(), n * sizeof(long long), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(ctx->pix_end.p, pix_end.data(), n * sizeof(long long), cudaMemcpyHostToDevice, stream));
+    // Pinned staging: [frames][ray ends][pixel ends][queue state].  The
+    // previous launch's copies out of it must have completed.
+    p.stage_bytes = n * sizeof(FrameParams) + 2 * n * sizeof(long long) + sizeof(QueueState);
+    CK(cudaEventSynchronize(ctx->stage_free));
+    if (p.stage_bytes > ctx->stage_cap) {
+        if (ctx->stage) CK(cudaFreeHost(ctx->stage));
+        ctx->stage = nullptr;
+        ctx->stage_cap = 0;
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&ctx->stage), p.stage_bytes, cudaHostAllocDefault));
+        ctx->stage_cap = p.stage_bytes;
+    }
+    unsigned char* s = ctx->stage;
+    std::memcpy(s, frames.data(), n * sizeof(FrameParams));
+    long long* ends = reinterpret_cast<long long*>(s + n * sizeof(FrameParams));
+    for (int i = 0; i < n; ++i) {
+        ends[i] = frames[i].ray_begin + frames[i].n_rays;
+        ends[n + i] = frames[i].pixel_begin + static_cast<long long>(frames[i].width) * frames[i].height;
+    }
     QueueState q;
     std::memset(&q, 0, sizeof q);
     q.budget = ctx->budget;
     q.abort = ctx->abort_requested.load() ? 1 : 0;
-    CK(cudaMemcpyAsync(ctx->d_queue, &q, sizeof q, cudaMemcpyHostToDevice, stream));
-    ctx->h2d += static_cast<long long>(n * sizeof(FrameParams) + 2 * n * sizeof(long long) + sizeof q);
+    std::memcpy(s + n * sizeof(FrameParams) + 2 * n * sizeof(long long), &q, sizeof q);
 
     const int prec = frames[0].precision_tag;
     const bh_launch_params& lp = ctx->launch[prec == BH_PRECISION_MIXED ? 1 : 0];
     const bh_launch_params& lp64 = ctx->launch[0];
     int bps = lp.blocks_per_sm > 0 ? lp.blocks_per_sm : trace_blocks_per_sm(prec, lp.block_size, lp.reg_variant == 2);
     if (bps < 1) bps = 1;
-    TraceLaunch tl;
+    TraceLaunch& tl = p.tl;
+    std::memset(&tl, 0, sizeof tl);
     tl.frames = static_cast<const FrameParams*>(ctx->frames.p);
     tl.frame_ray_end = static_cast<const long long*>(ctx->ray_end.p);
     tl.nframes = n;
@@ -240,7 +277,7 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     tl.rays_per_thread = lp.rays_per_thread;
     tl.refill = lp.refill;
     tl.budget = ctx->budget;
-    tl.deferred = mixed ? ctx->deferred.p : nullptr;
+    tl.deferred = p.mixed ? ctx->deferred.p : nullptr;
     tl.reg_variant = (lp.reg_variant == 2) ? 1 : 0;
     // The binary64 pass that finishes deferred mixed-precision rays runs with
     // the FP64 launch shape.
@@ -251,11 +288,9 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
         tl.grid_resume = ctx->sm_count * (bps64 < 1 ? 1 : bps64);
     }
     tl.resume_event = timed ? ctx->ev[3] : nullptr;
-    if (timed) CK(cudaEventRecord(ctx->ev[0], stream));
-    if (rays > 0) CK(launch_trace(tl, stream));
-    if (timed) CK(cudaEventRecord(ctx->ev[1], stream));
 
-    ShadeLaunch sl;
+    ShadeLaunch& sl = p.sl;
+    std::memset(&sl, 0, sizeof sl);
     sl.frames = tl.frames;
     sl.frame_pixel_end = static_cast<const long long*>(ctx->pix_end.p);
     sl.nframes = n;
@@ -266,10 +301,9 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     sl.rays = d_rays;
     sl.pixel_lum = static_cast<double*>(ctx->lum.p);
     sl.ray_class = nullptr;
-    CK(launch_shade(sl, stream));
-    if (timed) CK(cudaEventRecord(ctx->ev[2], stream));
 
-    ReduceLaunch rl;
+    ReduceLaunch& rl = p.rl;
+    std::memset(&rl, 0, sizeof rl);
     rl.frames = tl.frames;
     rl.nframes = n;
     rl.hits = tl.hits;
@@ -277,8 +311,40 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     rl.partials = static_cast<FrameStats*>(ctx->partials.p);
     rl.out = static_cast<FrameStats*>(ctx->fstats.p);
     rl.blocks_per_frame = kReduceBlocks;
-    CK(launch_reduce(rl, stream));
     return BH_OK;
+}
+
+// Stream half: staging -> device copies, then the kernels.  No allocation and
+// no host-synchronous call, so a CUDA graph can capture it.  Under capture the
+// caller records `stage_free` after the graph launch instead (an event
+// recorded during capture is not recorded again when the graph replays).
+int record_launch(bh_ctx* ctx, const Plan& p, cudaStream_t stream, bool timed, bool captured = false) {
+    const int n = p.n;
+    const unsigned char* s = ctx->stage;
+    CK(cudaMemcpyAsync(ctx->frames.p, s, n * sizeof(FrameParams), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->ray_end.p, s + n * sizeof(FrameParams), n * sizeof(long long),
+                       cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->pix_end.p, s + n * sizeof(FrameParams) + n * sizeof(long long),
+                       n * sizeof(long long), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->d_queue, s + n * sizeof(FrameParams) + 2 * n * sizeof(long long),
+                       sizeof(QueueState), cudaMemcpyHostToDevice, stream));
+    if (!captured) CK(cudaEventRecord(ctx->stage_free, stream));
+    if (timed) CK(cudaEventRecord(ctx->ev[0], stream));
+    if (p.rays > 0) CK(launch_trace(p.tl, stream));
+    if (timed) CK(cudaEventRecord(ctx->ev[1], stream));
+    CK(launch_shade(p.sl, stream));
+    if (timed) CK(cudaEventRecord(ctx->ev[2], stream));
+    CK(launch_reduce(p.rl, stream));
+    return BH_OK;
+}
+
+int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_ray_result* d_rays,
+            cudaStream_t stream, bool timed) {
+    Plan p;
+    int rc = plan_launch(ctx, frames, d_pixels, d_rays, timed, p);
+    if (rc != BH_OK) return rc;
+    ctx->h2d += static_cast<long long>(p.stage_bytes);
+    return record_launch(ctx, p, stream, timed);
 }
 
 // Read back the queue state and per-frame stats after the stream drained.
@@ -382,6 +448,7 @@ int bh_gpu_create(int device, bh_ctx** out) {
     *ctx->h_one = 1;
     for (auto& ev : ctx->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&ctx->stage_free, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     *out = ctx;
     return BH_OK;
 }
@@ -399,6 +466,9 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     cudaFree(ctx->d_bin_start);
     cudaFree(ctx->d_queue);
     if (ctx->h_one) cudaFreeHost(ctx->h_one);
+    if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+    if (ctx->stage) cudaFreeHost(ctx->stage);
+    if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
     for (auto& ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -499,8 +569,48 @@ int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz
     size_t npx = 0;
     for (int i = 0; i < n; ++i) npx += static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
     if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
-    rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true);
-    if (rc != BH_OK) return rc;
+    // The whole batch is one CUDA graph: staging copies, the persistent trace
+    // launch over every frame's rays (plus the binary64 pass), shading and the
+    // stats.  It is captured once per batch shape and replayed while the shape
+    // (frame count, sizes, buffers, launch shape) stays the same; the frame
+    // constants change freely, they are read from the pinned staging buffer.
+    Plan p;
+    if ((rc = plan_launch(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, false, p)) != BH_OK)
+        return rc;
+    ctx->h2d += static_cast<long long>(p.stage_bytes);
+    std::vector<unsigned char> key(sizeof p.tl + sizeof p.sl + sizeof p.rl + sizeof(void*) + sizeof(size_t));
+    {
+        unsigned char* k = key.data();
+        std::memcpy(k, &p.tl, sizeof p.tl); k += sizeof p.tl;
+        std::memcpy(k, &p.sl, sizeof p.sl); k += sizeof p.sl;
+        std::memcpy(k, &p.rl, sizeof p.rl); k += sizeof p.rl;
+        std::memcpy(k, &ctx->stage, sizeof(void*)); k += sizeof(void*);
+        std::memcpy(k, &p.stage_bytes, sizeof(size_t));
+    }
+    if (!ctx->batch_exec || key != ctx->batch_key) {
+        if (ctx->batch_exec) {
+            cudaGraphExecDestroy(ctx->batch_exec);
+            ctx->batch_exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const int rrc = record_launch(ctx, p, ctx->stream, false, true);
+        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (rrc != BH_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rrc;
+        }
+        CK(ce);
+        const cudaError_t ie = cudaGraphInstantiate(&ctx->batch_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(ie);
+        ctx->batch_key = key;
+    }
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(cudaGraphLaunch(ctx->batch_exec, ctx->stream));
+    CK(cudaEventRecord(ctx->stage_free, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     size_t off = 0;
     for (int i = 0; i < n; ++i) {
         const size_t m = static_cast<size_t>(cfgs[i].width) * cfgs[i].height;

@@ -1,0 +1,52 @@
+"""Frame sharding across ranks (one process per GPU).
+
+Rays never interact, so a multi-GPU render needs no data-path collective: each
+rank renders whole frames.  ``frames_for_rank`` partitions a list of frames
+into contiguous blocks of nearly equal ray count (the work unit), and
+``reduce_stats`` combines the per-rank ``RenderStats`` the way the reference
+combines its per-thread stats (render.cpp:481-494): counters summed, drift
+maxima maximised, ``seconds`` the maximum over ranks.  Both run over any
+torch.distributed process group (NCCL on GPUs, gloo on CPU).
+"""
+from __future__ import annotations
+
+from .config import RenderStats
+
+SUM_FIELDS = ("rays", "steps", "captured", "disc_hits", "sun_hits", "star_hits", "jet_rays",
+              "escaped", "exhausted", "total_flux", "attempts", "h2d_bytes", "d2h_bytes")
+MAX_FIELDS = ("max_norm_error", "max_carter_drift", "seconds", "kernel_ms", "shade_ms")
+
+
+def frames_for_rank(cfgs: list, rank: int, world: int) -> list:
+    """Indices of the frames rank `rank` of `world` renders: contiguous blocks
+    split at the ray-count quantiles (every frame on exactly one rank)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    weights = [c.n_rays for c in cfgs]
+    total = sum(weights)
+    out, acc = [], 0
+    for i, w in enumerate(weights):
+        # the frame goes to the rank owning the midpoint of its ray range
+        mid = acc + 0.5 * w
+        owner = min(world - 1, int(world * mid / total)) if total > 0 else i % world
+        if owner == rank:
+            out.append(i)
+        acc += w
+    return out
+
+
+def reduce_stats(stats: RenderStats, group=None, device=None) -> RenderStats:
+    """All-reduce one rank's stats into the job's (sum / max), on every rank."""
+    import torch
+    import torch.distributed as dist
+
+    s = torch.tensor([float(getattr(stats, f)) for f in SUM_FIELDS], dtype=torch.float64, device=device)
+    m = torch.tensor([float(getattr(stats, f)) for f in MAX_FIELDS], dtype=torch.float64, device=device)
+    dist.all_reduce(s, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX, group=group)
+    out = RenderStats()
+    for f, v in zip(SUM_FIELDS, s.tolist()):
+        setattr(out, f, v if f == "total_flux" else int(round(v)))
+    for f, v in zip(MAX_FIELDS, m.tolist()):
+        setattr(out, f, v)
+    return out

@@ -238,7 +238,11 @@ int  bh_gpu_trace_rays(bh_ctx* ctx, const bh_render_config* cfg,
 /* Many frames of any size in one persistent launch (replaces the serial frame
    loop of main.cpp:952-989).  outs[i] receives frame i's pixels; stats[i]
    (optional array) receives frame i's counters.  All frames must share the
-   precision, sky and star settings of cfgs[0]. */
+   precision, sky and star settings of cfgs[0].  The batch runs as one CUDA
+   graph (staging copies, trace, shade, stats), captured on the first call and
+   replayed while the batch shape (frame count and sizes, launch parameters,
+   buffers) is unchanged; kernel_ms is then the device time of the whole graph
+   and shade_ms is 0. */
 int  bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n,
                          bh_xyz* const* outs, bh_render_stats* stats);
 

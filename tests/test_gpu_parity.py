@@ -263,6 +263,29 @@ def test_batch_equals_single_frames(renderer):
         assert s.disc_hits == single.disc_hits
 
 
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+def test_batch_graph_replay_follows_new_frame_constants(renderer, precision):
+    """The batch graph is captured once per shape; a second batch of the same
+    shape with other cameras and spins replays it and must still match the
+    single-frame renders, and a change of shape recaptures."""
+    def batch(spin, incl):
+        cfgs = [kerr_a09_i60(width=32, height=24, spin=spin), kerr_a09_i60(width=24, height=32, spin=spin)]
+        for c in cfgs:
+            c.cam.theta = math.radians(incl)
+            c.precision = precision
+        return cfgs
+
+    for cfgs in (batch(0.9, 60.0), batch(0.5, 75.0), batch(0.99, 85.0)):
+        outs = renderer.render_batch(cfgs)
+        for c, o in zip(cfgs, outs):
+            assert np.array_equal(o, renderer.render(c))
+    grown = batch(0.7, 70.0) + [kerr_a09_i60(width=16, height=16, spin=0.7)]
+    grown[-1].precision = precision
+    outs = renderer.render_batch(grown)
+    for c, o in zip(grown, outs):
+        assert np.array_equal(o, renderer.render(c))
+
+
 def test_batch_rejects_mixed_catalogues(renderer):
     a = kerr_a09_i60(width=8, height=8)
     b = kerr_a09_i60(width=8, height=8, seed=5)

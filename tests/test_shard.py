@@ -1,0 +1,76 @@
+"""Multi-rank frame sharding and stats reduction, on CPU with gloo.
+
+The render path shards by frame with no data-path collective; the only
+cross-rank step is the stats reduction (sums and maxima) and the timing max.
+Two gloo ranks on 127.0.0.1 run the same code bench.py runs over NCCL.
+"""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from blackhole_b200 import shard, workloads
+from blackhole_b200.config import RenderStats
+
+
+def test_partition_covers_every_frame_once_and_balances_rays():
+    frames = workloads.batch_64_frames()
+    for world in (1, 2, 3, 4, 8):
+        parts = [shard.frames_for_rank(frames, r, world) for r in range(world)]
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(frames)))
+        rays = [sum(frames[i].n_rays for i in p) for p in parts]
+        biggest = max(f.n_rays for f in frames)
+        assert max(rays) - min(rays) <= 2 * biggest + 1
+
+
+def test_partition_rejects_bad_ranks():
+    with pytest.raises(ValueError):
+        shard.frames_for_rank(workloads.batch_64_frames(), 2, 2)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    st = RenderStats(rays=100 + rank, steps=1000 * (rank + 1), captured=rank, disc_hits=10, escaped=5,
+                     max_norm_error=1e-9 * (rank + 1), max_carter_drift=[3e-6, 1e-6][rank],
+                     seconds=0.5 + rank, total_flux=1.5 * (rank + 1), attempts=1001 * (rank + 1))
+    tot = shard.reduce_stats(st)
+    frames = workloads.batch_64_frames()
+    mine = shard.frames_for_rank(frames, rank, world)
+    q.put((rank, tot.as_tuple() if hasattr(tot, "as_tuple") else vars(tot), mine))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_reduce_stats_and_split_frames():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort(key=lambda t: t[0])
+    for _, tot, _ in res:
+        assert tot["rays"] == 201 and tot["steps"] == 3000 and tot["captured"] == 1
+        assert tot["disc_hits"] == 20 and tot["escaped"] == 10 and tot["attempts"] == 3003
+        assert tot["max_norm_error"] == pytest.approx(2e-9)
+        assert tot["max_carter_drift"] == pytest.approx(3e-6)
+        assert tot["seconds"] == pytest.approx(1.5) and tot["total_flux"] == pytest.approx(4.5)
+    a, b = res[0][2], res[1][2]
+    assert sorted(a + b) == list(range(64)) and not set(a) & set(b)
