@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--size", type=int, default=1024, help="frame side (default 1024)")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison leg")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batch", action="store_true", help="skip the 64-frame batch leg")
+    p.add_argument("--no-photon-ring", action="store_true", help="skip the 4096^2 photon-ring leg")
     p.add_argument("--once", action="store_true",
                    help="render the frame once in mixed precision and once in FP64 and exit (for ncu captures)")
     return p.parse_args()
@@ -196,12 +198,21 @@ def roofline(kernel_ms: float, steps: int, attempts: int, precision: str, peak: 
     }
 
 
-def accuracy(r, size, rank, world):
+def accuracy(r, size, rank, world, cfgs=None):
     """Per-ray error of the mixed frame against the FP64 frame (same rays)."""
     from blackhole_b200 import abi
 
-    a = r.trace_rays(frame_config(size, rank, world, abi.PRECISION_FP64))
-    b = r.trace_rays(frame_config(size, rank, world, abi.PRECISION_MIXED))
+    if cfgs is None:
+        cfgs = (frame_config(size, rank, world, abi.PRECISION_FP64),
+                frame_config(size, rank, world, abi.PRECISION_MIXED))
+    a = r.trace_rays(cfgs[0])
+    b = r.trace_rays(cfgs[1])
+    return compare_rays(a, b)
+
+
+def compare_rays(a, b):
+    from blackhole_b200 import abi
+
     same = a["what"] == b["what"]
     out = {"class_agree": float(same.mean()), "against": "the FP64 GPU frame (per ray)"}
     disc = same & (a["what"] == abi.HIT_DISC) & (a["g"] > 0)
@@ -217,6 +228,37 @@ def accuracy(r, size, rank, world):
     return out
 
 
+def photon_ring_leg(r, torch, flush, barrier, world, rank):
+    """4096^2 frame of +-8 M centred on the prograde equatorial point of the
+    critical curve (a = 0.998, 75 deg): mixed and FP64 device time, the
+    per-ray step-count distribution and the mixed-vs-FP64 error."""
+    from blackhole_b200 import abi, workloads
+
+    cm = workloads.photon_ring_4096(abi.PRECISION_MIXED)
+    cd = workloads.photon_ring_4096(abi.PRECISION_FP64)
+    for c in (cm, cd):
+        c.cam.phi = 2.0 * math.pi * rank / max(1, world)
+    t_m, _, st_m, _ = time_device(r, cm, 2, 1, torch, flush, barrier)
+    t_d, _, st_d, _ = time_device(r, cd, 2, 1, torch, flush, barrier)
+    out = {"workload": "photon_ring_4096: a=0.998, inclination 75 deg, 4096x4096, +-8 M centred (yaw) on "
+                       "alpha=-2.18 M, disc r_isco..100 M at 0.5 Eddington, M=6.5e9 M_sun",
+           "rays": cm.n_rays,
+           "mixed": {"value": round(cm.n_rays * 2 / (t_m * 1e-3), 1), "unit": "rays/s", "ms": round(t_m / 2, 3),
+                     "steps_per_ray": round(st_m.steps / st_m.rays, 2)},
+           "fp64": {"value": round(cd.n_rays * 2 / (t_d * 1e-3), 1), "unit": "rays/s", "ms": round(t_d / 2, 3),
+                    "steps_per_ray": round(st_d.steps / st_d.rays, 2)}}
+    out["mixed_over_fp64"] = round(out["mixed"]["value"] / out["fp64"]["value"], 3)
+    a = r.trace_rays(cd)
+    b = r.trace_rays(cm)
+    steps = a["steps"].ravel()
+    out["fp64_steps"] = {"mean": float(steps.mean()), "p50": float(np.quantile(steps, .5)),
+                         "p99": float(np.quantile(steps, .99)), "max": int(steps.max()),
+                         "frac_gt_2000": float((steps > 2000).mean())}
+    out["classes"] = {abi.HIT_NAMES[k]: int(v) for k, v in enumerate(np.bincount(a["what"].ravel(), minlength=6))}
+    out["accuracy"] = compare_rays(a, b)
+    return out
+
+
 def cpu_baseline(size: int, max_seconds: float = 20.0):
     """The reference CPU path on a bounded sample of the frame's rows."""
     import oracle
@@ -229,7 +271,7 @@ def cpu_baseline(size: int, max_seconds: float = 20.0):
         # The reference has one sky and one stop rule: run its own.
         cfg.sky_mode = abi.SKY_GALACTIC
         cfg.stop_mode = abi.STOP_REFERENCE
-        rows = list(range(0, cfg.height, 16))
+        rows = list(range(0, cfg.height, 2))
         t0 = time.perf_counter()
         _, st, setup = ref.render_rows(cfg, rows, threads)
         wall = time.perf_counter() - t0 - setup
@@ -246,6 +288,39 @@ def cpu_baseline(size: int, max_seconds: float = 20.0):
     return {"value": st.rays / dt, "unit": "rays/s", "cores": 1, "kind": "port",
             "sample": f"{st.rays} rays of a {w}x8 window at the frame centre, oracle port, 1 thread",
             "seconds": dt}
+
+
+def batch_leg(r, rank, world, barrier, max_over_ranks, steps=2, warmup=1):
+    """The 64-frame batch (uneven sizes 256^2..2048^2, 89.1 M rays) through
+    bh_gpu_render_batch: one persistent launch over all frames, captured as a
+    CUDA graph on the first call and replayed.  Frames are split across ranks
+    by ray count; the job's rate is all rays over the slowest rank."""
+    from blackhole_b200 import shard, workloads
+
+    frames = workloads.batch_64_frames()
+    mine = [frames[i] for i in shard.frames_for_rank(frames, rank, world)]
+    rays = sum(c.n_rays for c in frames)
+    for _ in range(warmup):
+        r.render_batch(mine)
+    barrier()
+    dev_ms, wall = 0.0, 0.0
+    st = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        r.render_batch(mine, st)
+        wall += time.perf_counter() - t0
+        dev_ms += st[0].kernel_ms if st else 0.0
+    dev_ms = max_over_ranks(dev_ms)
+    wall = max_over_ranks(wall)
+    return {"workload": "batch_64_frames: spins {0,0.5,0.9,0.998} x inclinations {15,45,70,85} deg x "
+                        "{256,512,1024,2048}^2, r_obs uniform 500..2000 M, mixed precision",
+            "frames": len(frames), "rays_per_step": rays, "steps": steps, "warmup": warmup,
+            "value": round(rays * steps / (dev_ms * 1e-3), 1) if dev_ms > 0 else None, "unit": "rays/s",
+            "ms_per_step": round(dev_ms / steps, 3),
+            "timing": "device time of the captured graph (staging copies, trace, shade, stats), max over ranks",
+            "e2e": {"value": round(rays * steps / wall, 1), "unit": "rays/s",
+                    "api": "bh_gpu_render_batch into pageable host arrays, wall clock"},
+            "steps_per_ray": round(sum(s.steps for s in st) / max(1, sum(s.rays for s in st)), 2)}
 
 
 def gpu_arm(args):
@@ -346,9 +421,22 @@ def gpu_arm(args):
                   "h2d_bytes_per_step": int(st_e.h2d_bytes), "d2h_bytes_per_step": int(st_e.d2h_bytes),
                   "api": "bh_gpu_render (C-ABI) into pinned host memory, wall clock"}
 
-    # Kernels of ours launched in the timed region: trace, shade, 2 reduce per step.
-    out["gpu_launches"] = 4 * args.steps
+    # Kernels of ours launched in the timed region per mixed step: trace,
+    # binary64 resume trace, shade, 2 reduce.
+    out["gpu_launches"] = 5 * args.steps
     out["clocks"] = clk.summary()
+
+    if not args.no_photon_ring:
+        try:
+            out["photon_ring"] = photon_ring_leg(r, torch, flush, barrier, world, rank)
+        except Exception as e:  # reported, not hidden
+            out["photon_ring"] = {"error": repr(e)}
+
+    if not args.no_batch:
+        try:
+            out["batch"] = batch_leg(r, rank, world, barrier, max_over_ranks)
+        except Exception as e:  # reported, not hidden
+            out["batch"] = {"error": repr(e)}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -382,7 +470,7 @@ def reference_arm(args):
         cfg.sky_mode = abi.SKY_GALACTIC
         cfg.stop_mode = abi.STOP_REFERENCE
     # Each step: a bounded sample of rows (disjoint row sets cycle through the frame).
-    rows_per_step = 16
+    rows_per_step = 64
     stride = max(1, cfg.height // rows_per_step)
 
     def step(i):

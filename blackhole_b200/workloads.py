@@ -101,17 +101,57 @@ def adjoint_512(target: bool = False) -> RenderConfig:
     )
 
 
+def critical_curve_prograde_edge(a: float, inclination: float) -> float:
+    """Image-plane abscissa (in M, Bardeen's alpha = -xi / sin i) where the
+    critical curve of a Kerr hole of spin a seen from inclination i crosses the
+    equator line on the prograde side: the spherical photon orbit radius r_p
+    in [r_ph+, r_ph-] with beta^2 = eta + a^2 cos^2 i - xi^2 cot^2 i = 0,
+    xi = -(r^3 - 3 r^2 + a^2 r + a^2) / (a (r - 1)),
+    eta = -r^3 (r^3 - 6 r^2 + 9 r - 4 a^2) / (a^2 (r - 1)^2)  (Bardeen 1973).
+    Negative: on the camera's left, where prograde photons pass."""
+    aa = abs(a)
+    if aa < 1e-6:
+        return -math.sqrt(27.0)
+    r_lo = 2.0 * (1.0 + math.cos((2.0 / 3.0) * math.acos(-aa)))
+    r_hi = 2.0 * (1.0 + math.cos((2.0 / 3.0) * math.acos(aa)))
+
+    def xi(r):
+        return -(r ** 3 - 3.0 * r * r + aa * aa * r + aa * aa) / (aa * (r - 1.0))
+
+    def beta2(r):
+        eta = -r ** 3 * (r ** 3 - 6.0 * r * r + 9.0 * r - 4.0 * aa * aa) / (aa * aa * (r - 1.0) ** 2)
+        return eta + aa * aa * math.cos(inclination) ** 2 - xi(r) ** 2 / math.tan(inclination) ** 2
+
+    # beta^2 < 0 just above r_ph+ and > 0 inside the curve: scan for the
+    # first sign change, then bisect.
+    n = 4000
+    prev_r, prev_v = r_lo + 1e-9, beta2(r_lo + 1e-9)
+    for k in range(1, n + 1):
+        r = r_lo + (r_hi - r_lo) * k / n
+        v = beta2(r)
+        if (v > 0.0) != (prev_v > 0.0):
+            lo, hi = prev_r, r
+            for _ in range(100):
+                mid = 0.5 * (lo + hi)
+                if (beta2(mid) > 0.0) == (prev_v > 0.0):
+                    lo = mid
+                else:
+                    hi = mid
+            return -xi(0.5 * (lo + hi)) / math.sin(inclination) * (1.0 if a >= 0 else -1.0)
+        prev_r, prev_v = r, v
+    raise ValueError("no equatorial point of the critical curve")
+
+
 def photon_ring_4096(precision: int = abi.PRECISION_MIXED, size: int = 4096) -> RenderConfig:
     """Narrow +-8 M frame at a = 0.998, inclination 75 deg, M = 6.5e9 M_sun,
-    disc r_isco..100 M at 0.5 Eddington, aimed (yaw) at the prograde edge of
-    the critical curve so many rays orbit before escaping or falling in."""
+    disc r_isco..100 M at 0.5 Eddington, centred (yaw) on the prograde
+    equatorial point of the critical curve (alpha = -2.18 M), where rays
+    skim the photon orbits before escaping, falling in or meeting the disc."""
     cfg = _base(
         M_kg=6.5e9 * M_SUN, spin=0.998,
         cam=Camera(r=R_OBS, theta=math.radians(75.0), phi=0.0, fov=_fov(8.0)),
         width=size, height=size, disc_r_out=100.0, eddington=0.5,
         precision=precision,
     )
-    # The prograde photon orbit of a = 0.998 sits at about b = 2.2 M on the
-    # approaching side; centre the frame there.
-    cfg.cam.yaw = math.atan(-2.2 / R_OBS)
+    cfg.cam.yaw = math.atan(critical_curve_prograde_edge(0.998, math.radians(75.0)) / R_OBS)
     return cfg
