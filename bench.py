@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true", help="skip the 64-frame batch leg")
     p.add_argument("--no-photon-ring", action="store_true", help="skip the 4096^2 photon-ring leg")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the 512^2 adjoint leg")
     p.add_argument("--once", action="store_true",
                    help="render the frame once in mixed precision and once in FP64 and exit (for ncu captures)")
     return p.parse_args()
@@ -323,6 +324,36 @@ def batch_leg(r, rank, world, barrier, max_over_ranks, steps=2, warmup=1):
             "steps_per_ray": round(sum(s.steps for s in st) / max(1, sum(s.rays for s in st)), 2)}
 
 
+def adjoint_leg(r, steps=3, warmup=1):
+    """Gradients per second of the discrete adjoint on the 512^2 gradient
+    workload: one gradient = the binary64 render, the loss against the target
+    frame and d(loss)/d(spin, inclination, Eddington ratio, r_out)."""
+    from blackhole_b200 import workloads
+
+    cfg = workloads.adjoint_512()
+    target = r.render(workloads.adjoint_512(target=True))[..., 1].astype(np.float32)
+    for _ in range(warmup):
+        r.adjoint(cfg, target)
+    dev_ms, gs = [], None
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        gs = r.adjoint(cfg, target)
+        dev_ms.append(gs["kernel_ms"])
+    wall = time.perf_counter() - t0
+    ms = sum(dev_ms) / len(dev_ms)
+    return {"workload": "adjoint_512: a=0.7, inclination 50 deg, 0.2 Eddington, r_out 25 M, 512x512, binary64; "
+                        "target rendered at a=0.75, 53 deg, 0.22, 27 M; checkpoints every 16 accepted steps",
+            "value": round(1e3 / ms, 2), "unit": "grads/s", "ms_per_grad": round(ms, 3),
+            "timing": "device time of render + adjoint + reductions (CUDA events), mean of "
+                      f"{steps} after {warmup} warm-up",
+            "e2e": {"value": round(steps / wall, 2), "unit": "grads/s",
+                    "api": "bh_gpu_adjoint from host target to host gradient, wall clock"},
+            "loss": gs["loss"], "grad": [gs["d_spin"], gs["d_inclination"], gs["d_eddington"], gs["d_r_out"]],
+            "steps_per_ray": round(gs["steps"] / gs["rays"], 2),
+            "replay_over_forward": round(gs["replayed_steps"] / max(1, gs["steps"]), 3),
+            "disc_rays": gs["disc_rays"], "sky_rays": gs["sky_rays"]}
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -425,6 +456,12 @@ def gpu_arm(args):
     # binary64 resume trace, shade, 2 reduce.
     out["gpu_launches"] = 5 * args.steps
     out["clocks"] = clk.summary()
+
+    if not args.no_adjoint:
+        try:
+            out["adjoint"] = adjoint_leg(r)
+        except Exception as e:  # reported, not hidden
+            out["adjoint"] = {"error": repr(e)}
 
     if not args.no_photon_ring:
         try:

@@ -146,6 +146,19 @@ class bh_trace_record(C.Structure):
 NOALLOC_MAX_RAYS = 65536
 
 
+class bh_grad4(C.Structure):
+    _fields_ = [
+        ("loss", C.c_double), ("d_spin", C.c_double), ("d_inclination", C.c_double),
+        ("d_eddington", C.c_double), ("d_r_out", C.c_double), ("kernel_ms", C.c_double),
+        ("rays", C.c_longlong), ("steps", C.c_longlong), ("replayed_steps", C.c_longlong),
+        ("disc_rays", C.c_longlong), ("sky_rays", C.c_longlong),
+        ("max_checkpoint_interval", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
 def trace_record_dtype():
     import numpy as np
 

@@ -65,7 +65,40 @@ def build(verbose: bool = False, force: bool = False) -> str:
             raise RuntimeError("nvcc link failed")
         if verbose:
             print(f"linked {LIB}")
+    build_check(verbose=verbose, force=force)
     return LIB
+
+
+# Test harness library: the adjoint's per-ray code compiled for the host (the
+# tests check its mathematics on a CPU); never loaded by the render library.
+CHECK_LIB = os.path.join(HERE, "lib", "libbh_adjoint_check.so")
+
+
+def build_check(verbose: bool = False, force: bool = False) -> str:
+    srcs = [os.path.join(CSRC, "check", "bh_adjoint_check.cu"), os.path.join(CSRC, "bh_scene.cpp"),
+            os.path.join(CSRC, "bh_adjoint_frame.cpp")]
+    hdrs = _deps()
+    objs = []
+    for s in srcs:
+        o = os.path.join(BUILD, "check_" + os.path.basename(s) + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            cmd = [NVCC] + ARCH + COMMON + ["-c", s, "-o", o]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise RuntimeError(f"nvcc failed on {s}")
+            if verbose:
+                print(f"compiled {os.path.basename(s)} (check)")
+    if force or _stale(CHECK_LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", CHECK_LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc link failed (check library)")
+        if verbose:
+            print(f"linked {CHECK_LIB}")
+    return CHECK_LIB
 
 
 if __name__ == "__main__":

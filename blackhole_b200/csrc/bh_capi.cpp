@@ -17,6 +17,7 @@
 
 #include "../../include/bh_gpu.h"
 #include "bh_frame.h"
+#include "bh_adjoint.h"
 #include "bh_launch.h"
 #include "bh_scene.h"
 
@@ -57,6 +58,9 @@ struct bh_ctx {
     HostSky sky_meta;
 
     DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats, deferred;
+    // Adjoint: target image, per-ray gradients and luminances, checkpoint
+    // slots, counters and the five sums.
+    DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums;
     QueueState* d_queue = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     long long h2d = 0, d2h = 0;          // bytes copied by the current call
@@ -458,7 +462,8 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end, &ctx->deferred,
-                      &ctx->pix_end, &ctx->partials, &ctx->fstats})
+                      &ctx->pix_end, &ctx->partials, &ctx->fstats, &ctx->adj_target, &ctx->adj_grad, &ctx->adj_Y,
+                      &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums})
         if (b->p) cudaFree(b->p);
     cudaFree(ctx->d_table);
     cudaFree(ctx->d_star_pos);
@@ -622,6 +627,103 @@ int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz
     CK(cudaStreamSynchronize(ctx->stream));
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return finish(ctx, n, stats, nullptr, true, secs);
+}
+
+// The binary64 render of `cfg` (its loss against `target`) and the discrete
+// adjoint of that loss; per-ray gradients and luminances on request.
+static int adjoint_impl(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out,
+                        double* ray_grad, double* ray_Y) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!target || !out) return fail(ctx, BH_ERR_INVALID_ARG, "target and out must not be NULL");
+    int rc = check_cfg_header(ctx, cfg);
+    if (rc != BH_OK) return rc;
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    bh_render_config c = *cfg;
+    c.precision = BH_PRECISION_FP64;       // the adjoint differentiates the binary64 path
+    std::vector<FrameParams> frames;
+    if ((rc = prepare_frames(ctx, &c, 1, frames)) != BH_OK) return rc;
+    AdjointFrame X;
+    {
+        std::string err;
+        if ((rc = make_adjoint_frame(c, frames[0], X, err)) != BH_OK) return fail(ctx, rc, err);
+    }
+    const int block = 128;
+    int bps = adjoint_blocks_per_sm(block);
+    if (bps < 1) bps = 1;
+    const int grid = ctx->sm_count * bps;
+    const size_t npx = static_cast<size_t>(c.width) * c.height;
+    const long long n_rays = frames[0].n_rays;
+    if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->adj_target, npx * sizeof(float))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->adj_grad, static_cast<size_t>(n_rays) * 4 * sizeof(double))) != BH_OK) return rc;
+    if (ray_Y && (rc = ensure(ctx, ctx->adj_Y, static_cast<size_t>(n_rays) * sizeof(double))) != BH_OK) return rc;
+    const size_t ck_bytes = static_cast<size_t>(grid) * block * X.checkpoint_slots * 8 * sizeof(double);
+    if ((rc = ensure(ctx, ctx->adj_ckpt, ck_bytes)) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->adj_counters, 6 * sizeof(unsigned long long))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->adj_sums, 5 * sizeof(double))) != BH_OK) return rc;
+
+    CK(cudaMemcpyAsync(ctx->adj_target.p, target, npx * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += static_cast<long long>(npx * sizeof(float));
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    if ((rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, false)) != BH_OK)
+        return rc;
+    CK(cudaMemsetAsync(ctx->adj_counters.p, 0, 6 * sizeof(unsigned long long), ctx->stream));
+    AdjointLaunch L;
+    std::memset(&L, 0, sizeof L);
+    L.frame = frames[0];
+    L.X = X;
+    L.sky = sky_data(ctx);
+    L.pixels = static_cast<const bh_xyz*>(ctx->pixels.p);
+    L.target = static_cast<const float*>(ctx->adj_target.p);
+    L.ray_grad = static_cast<double*>(ctx->adj_grad.p);
+    L.ray_Y = ray_Y ? static_cast<double*>(ctx->adj_Y.p) : nullptr;
+    L.ckpt = static_cast<double*>(ctx->adj_ckpt.p);
+    L.counters = static_cast<unsigned long long*>(ctx->adj_counters.p);
+    L.sums = static_cast<double*>(ctx->adj_sums.p);
+    L.n_rays = n_rays;
+    L.grid = grid;
+    L.block = block;
+    CK(launch_adjoint(L, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    double sums[5];
+    unsigned long long cnt[6];
+    CK(cudaMemcpyAsync(sums, ctx->adj_sums.p, sizeof sums, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(cnt, ctx->adj_counters.p, sizeof cnt, cudaMemcpyDeviceToHost, ctx->stream));
+    if (ray_grad)
+        CK(cudaMemcpyAsync(ray_grad, ctx->adj_grad.p, static_cast<size_t>(n_rays) * 4 * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+    if (ray_Y)
+        CK(cudaMemcpyAsync(ray_Y, ctx->adj_Y.p, static_cast<size_t>(n_rays) * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if ((rc = finish(ctx, 1, nullptr, nullptr, false, secs)) != BH_OK) return rc;
+    std::memset(out, 0, sizeof *out);
+    out->loss = sums[0];
+    out->d_spin = sums[1];
+    out->d_inclination = sums[2];
+    out->d_eddington = sums[3];
+    out->d_r_out = sums[4];
+    out->kernel_ms = ms;
+    out->rays = n_rays;
+    out->steps = static_cast<long long>(cnt[1]);
+    out->replayed_steps = static_cast<long long>(cnt[2]);
+    out->disc_rays = static_cast<long long>(cnt[3]);
+    out->sky_rays = static_cast<long long>(cnt[4]);
+    out->max_checkpoint_interval = static_cast<int32_t>(cnt[5]);
+    return BH_OK;
+}
+
+int bh_gpu_adjoint(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out) {
+    return adjoint_impl(ctx, cfg, target, out, nullptr, nullptr);
+}
+
+int bh_gpu_adjoint_rays(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out,
+                        double* ray_grad, double* ray_Y) {
+    return adjoint_impl(ctx, cfg, target, out, ray_grad, ray_Y);
 }
 
 int bh_gpu_set_launch(bh_ctx* ctx, int precision, const bh_launch_params* p) {

@@ -1,4 +1,5 @@
-// bh_common.cuh - Device helpers shared by the trace and shade kernels.
+// bh_common.cuh - Helpers shared by the trace, shade and adjoint kernels (the
+// arithmetic ones also compile for the host).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,29 +12,29 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr unsigned kFull = 0xffffffffu;
 
 // std::max / std::min / std::clamp semantics (NaN handling included).
-__device__ __forceinline__ double dmaxr(double a, double b) { return (a < b) ? b : a; }
-__device__ __forceinline__ double dminr(double a, double b) { return (b < a) ? b : a; }
-__device__ __forceinline__ double dclamp(double v, double lo, double hi) {
+__host__ __device__ __forceinline__ double dmaxr(double a, double b) { return (a < b) ? b : a; }
+__host__ __device__ __forceinline__ double dminr(double a, double b) { return (b < a) ? b : a; }
+__host__ __device__ __forceinline__ double dclamp(double v, double lo, double hi) {
     return (v < lo) ? lo : (hi < v) ? hi : v;
 }
 
 // splitmix64 output of state z (scene.h:30-36) and its 53-bit uniform (scene.h:37).
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
 }
-__device__ __forceinline__ double u53(uint64_t z) { return (double)(z >> 11) * 0x1.0p-53; }
+__host__ __device__ __forceinline__ double u53(uint64_t z) { return (double)(z >> 11) * 0x1.0p-53; }
 
 // Pixel of a frame-local pixel index.  Pixels are enumerated in bands of four
 // rows, column by column inside a band, so that 32 consecutive rays cover an
 // 8 x 4 patch of the image (coherent paths) rather than 32 pixels of one row.
-__device__ __forceinline__ void pixel_xy(int W, int H, long long p, int* x, int* y) {
+__host__ __device__ __forceinline__ void pixel_xy(int W, int H, long long p, int* x, int* y) {
     const long long band_px = 4LL * W;
     const int band = (int)(p / band_px);
     const int rel = (int)(p - (long long)band * band_px);
     const int y0 = 4 * band;
-    const int bh = min(4, H - y0);
+    const int bh = (H - y0 < 4) ? H - y0 : 4;
     *x = rel / bh;
     *y = y0 + rel % bh;
 }

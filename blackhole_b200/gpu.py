@@ -66,6 +66,9 @@ def load_library():
             "bh_blackbody_table": (C.c_int, [P(C.c_double)]),
             "bh_gpu_fma_peak": (C.c_int, [C.c_int, C.c_int, P(C.c_double)]),
             "bh_gpu_trace_noalloc": (C.c_int, [C.c_int, cfg_p, C.c_void_p, C.c_void_p]),
+            "bh_gpu_adjoint": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4)]),
+            "bh_gpu_adjoint_rays": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4), P(C.c_double),
+                                              P(C.c_double)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(lib, name)
@@ -183,6 +186,31 @@ class Renderer:
                 stats.append(r)
         self._check(rc)
         return outs
+
+    # -- discrete adjoint ----------------------------------------------------------
+    def adjoint(self, cfg, target, per_ray: bool = False):
+        """Loss sum((Y - target)^2) over the pixels of the binary64 frame of
+        `cfg` (Y = CIE Y, W m^-2 sr^-1) and its gradient with respect to
+        (spin, inclination, eddington, r_out), as a dict (bh_grad4's fields).
+        With per_ray: also each ray's gradient contribution, shape
+        (n_rays, 4), and luminance, shape (n_rays,), in trace_rays order."""
+        c = _as_c(cfg)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        if t.size != c.width * c.height:
+            raise ValueError("target must hold width * height luminances")
+        g = abi.bh_grad4()
+        fp = C.POINTER(C.c_float)
+        dp = C.POINTER(C.c_double)
+        if not per_ray:
+            self._check(self.lib.bh_gpu_adjoint(self._h, C.byref(c), t.ctypes.data_as(fp), C.byref(g)))
+            return g.as_dict()
+        s = max(1, c.sqrt_spp)
+        n = c.width * c.height * s * s
+        rg = np.empty((n, 4), dtype=np.float64)
+        ry = np.empty(n, dtype=np.float64)
+        self._check(self.lib.bh_gpu_adjoint_rays(self._h, C.byref(c), t.ctypes.data_as(fp), C.byref(g),
+                                                 rg.ctypes.data_as(dp), ry.ctypes.data_as(dp)))
+        return g.as_dict(), rg, ry
 
     # -- launch control ----------------------------------------------------------
     def set_launch(self, block_size=0, rays_per_thread=0, refill=0, blocks_per_sm=0, reg_variant=0,

@@ -310,6 +310,45 @@ typedef struct bh_trace_record {
    Returns once the work is enqueued.  No counterpart in the reference. */
 int  bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_trace_record* d_out, void* stream);
 
+/* Result of the discrete adjoint (bh_gpu_adjoint). */
+typedef struct bh_grad4 {
+    double loss;             /* sum over pixels of (Y - target)^2, Y the CIE Y of the frame */
+    double d_spin;           /* dLoss / d(spin)                                   */
+    double d_inclination;    /* dLoss / d(camera polar angle cam.theta), per radian */
+    double d_eddington;      /* dLoss / d(eddington)                              */
+    double d_r_out;          /* dLoss / d(disc_r_out): 0 (see bh_gpu_adjoint)      */
+    double kernel_ms;        /* device time of the render, adjoint and reductions */
+    long long rays;
+    long long steps;         /* accepted steps of the adjoint's forward pass      */
+    long long replayed_steps;/* accepted steps recomputed by the reverse pass     */
+    long long disc_rays;
+    long long sky_rays;
+    int32_t max_checkpoint_interval;
+    int32_t reserved;
+} bh_grad4;
+
+/* The luminance loss of `cfg` against `target` (W*H floats, row-major, the
+   CIE Y in W m^-2 sr^-1 of each pixel) and its gradient with respect to the
+   spin, the camera inclination, the Eddington ratio and the disc's outer
+   radius.  The frame is rendered in binary64 (whatever cfg->precision says);
+   the gradient is the discrete adjoint of that render: each ray's accepted
+   DP5 step sequence is replayed backwards from checkpoints (every 16 accepted
+   steps, 64 per ray in flight; the interval doubles for longer rays), with
+   the step sizes and each ray's termination class held fixed.  The
+   luminance of a point-sampled frame changes with r_out only where a
+   sample's disc crossing passes the edge, so d_r_out is 0: the edges of the
+   disc and of the shadow act on finite differences of the frame through the
+   samples that change class, a boundary term the per-ray adjoint does not
+   contain.  Scenes with the Sun, a neutron star, a hot spot or a jet return
+   BH_ERR_UNSUPPORTED.  No counterpart in the reference. */
+int  bh_gpu_adjoint(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out);
+
+/* bh_gpu_adjoint plus, when not NULL, each ray's gradient contribution
+   (4 doubles: spin, inclination, eddington, r_out) and its luminance, in
+   bh_gpu_trace_rays order (pixel row-major, then sample). */
+int  bh_gpu_adjoint_rays(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out,
+                         double* ray_grad, double* ray_Y);
+
 /* Measured FMA throughput of `device` in TFLOP/s (2 FLOP per FMA) for
    BH_PRECISION_FP64 (binary64) or BH_PRECISION_MIXED (binary32): the ALU
    roofline of the trace kernel.  Extension; no counterpart in the reference. */
