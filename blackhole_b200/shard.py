@@ -5,8 +5,10 @@ rank renders whole frames.  ``frames_for_rank`` partitions a list of frames
 into contiguous blocks of nearly equal ray count (the work unit), and
 ``reduce_stats`` combines the per-rank ``RenderStats`` the way the reference
 combines its per-thread stats (render.cpp:481-494): counters summed, drift
-maxima maximised, ``seconds`` the maximum over ranks.  Both run over any
-torch.distributed process group (NCCL on GPUs, gloo on CPU).
+maxima maximised, ``seconds`` the maximum over ranks.  ``reduce_grads`` sums
+the adjoint's loss and four gradients over ranks that each differentiated
+their own frames (the loss of a set of frames is the sum of theirs).  All run
+over any torch.distributed process group (NCCL on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
@@ -49,4 +51,22 @@ def reduce_stats(stats: RenderStats, group=None, device=None) -> RenderStats:
         setattr(out, f, v if f == "total_flux" else int(round(v)))
     for f, v in zip(MAX_FIELDS, m.tolist()):
         setattr(out, f, v)
+    return out
+
+
+GRAD_FIELDS = ("loss", "d_spin", "d_inclination", "d_eddington", "d_r_out")
+
+
+def reduce_grads(grad: dict, group=None, device=None) -> dict:
+    """Sum-all-reduce of one rank's adjoint result (loss and the four
+    gradients; counters summed too), on every rank."""
+    import torch
+    import torch.distributed as dist
+
+    keys = GRAD_FIELDS + ("rays", "steps", "replayed_steps", "disc_rays", "sky_rays")
+    t = torch.tensor([float(grad.get(k, 0.0)) for k in keys], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    out = dict(grad)
+    for k, v in zip(keys, t.tolist()):
+        out[k] = v if k in GRAD_FIELDS else int(round(v))
     return out

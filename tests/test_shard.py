@@ -49,7 +49,9 @@ def _worker(rank, world, port, q):
     tot = shard.reduce_stats(st)
     frames = workloads.batch_64_frames()
     mine = shard.frames_for_rank(frames, rank, world)
-    q.put((rank, tot.as_tuple() if hasattr(tot, "as_tuple") else vars(tot), mine))
+    g = shard.reduce_grads({"loss": 1.0 + rank, "d_spin": [0.5, -2.0][rank], "d_inclination": 3.0,
+                            "d_eddington": 1e20 * (rank + 1), "d_r_out": 0.0, "rays": 10, "steps": 7})
+    q.put((rank, tot.as_tuple() if hasattr(tot, "as_tuple") else vars(tot), mine, g))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -66,7 +68,9 @@ def test_two_gloo_ranks_reduce_stats_and_split_frames():
         p.join(timeout=60)
         assert p.exitcode == 0
     res.sort(key=lambda t: t[0])
-    for _, tot, _ in res:
+    for _, tot, _, g in res:
+        assert g["loss"] == 3.0 and g["d_spin"] == -1.5 and g["d_inclination"] == 6.0
+        assert g["d_eddington"] == pytest.approx(3e20) and g["rays"] == 20 and g["steps"] == 14
         assert tot["rays"] == 201 and tot["steps"] == 3000 and tot["captured"] == 1
         assert tot["disc_hits"] == 20 and tot["escaped"] == 10 and tot["attempts"] == 3003
         assert tot["max_norm_error"] == pytest.approx(2e-9)
