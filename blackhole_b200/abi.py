@@ -33,6 +33,9 @@ STATUS_NAMES = {
 
 # Termination classes, in the order of Hit::What (render.cpp:37).
 HIT_HORIZON, HIT_DISC, HIT_SUN, HIT_STAR, HIT_SKY, HIT_EXHAUSTED = range(6)
+# Display tone curves, in img::ToneMap order (image.h:16).
+TONEMAP_LINEAR, TONEMAP_REINHARD, TONEMAP_ACES, TONEMAP_LOG, TONEMAP_HDR = range(5)
+TONEMAP_NAMES = ("linear", "reinhard", "aces", "log", "hdr")
 HIT_NAMES = ("Horizon", "Disc", "Sun", "Star", "Sky", "Exhausted")
 
 PRECISION_FP64 = 0
@@ -144,6 +147,14 @@ class bh_trace_record(C.Structure):
 
 
 NOALLOC_MAX_RAYS = 65536
+
+
+class bh_display(C.Structure):
+    _fields_ = [
+        ("exposure", C.c_double), ("key", C.c_double), ("glare", C.c_double),
+        ("glare_radius", C.c_double), ("log_decades", C.c_double),
+        ("tonemap", C.c_int32), ("reserved", C.c_int32),
+    ]
 
 
 class bh_grad4(C.Structure):

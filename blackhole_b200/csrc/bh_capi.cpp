@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -18,6 +19,7 @@
 #include "../../include/bh_gpu.h"
 #include "bh_frame.h"
 #include "bh_adjoint.h"
+#include "bh_display.h"
 #include "bh_launch.h"
 #include "bh_scene.h"
 
@@ -61,6 +63,8 @@ struct bh_ctx {
     // Adjoint: target image, per-ray gradients and luminances, checkpoint
     // slots, counters and the five sums.
     DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums;
+    // Display transform: blur scratch, glare weights, meter state, 8-bit output.
+    DevBuf disp_tmp, disp_near, disp_far, disp_k, disp_state, disp_rgb;
     QueueState* d_queue = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     long long h2d = 0, d2h = 0;          // bytes copied by the current call
@@ -463,7 +467,8 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end, &ctx->deferred,
                       &ctx->pix_end, &ctx->partials, &ctx->fstats, &ctx->adj_target, &ctx->adj_grad, &ctx->adj_Y,
-                      &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums})
+                      &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums, &ctx->disp_tmp, &ctx->disp_near,
+                      &ctx->disp_far, &ctx->disp_k, &ctx->disp_state, &ctx->disp_rgb})
         if (b->p) cudaFree(b->p);
     cudaFree(ctx->d_table);
     cudaFree(ctx->d_star_pos);
@@ -715,6 +720,118 @@ static int adjoint_impl(bh_ctx* ctx, const bh_render_config* cfg, const float* t
     out->sky_rays = static_cast<long long>(cnt[4]);
     out->max_checkpoint_interval = static_cast<int32_t>(cnt[5]);
     return BH_OK;
+}
+
+// The display transform of the frame in ctx->pixels (W x H, device), on
+// ctx->stream; copies the 8-bit image and the exposure back and synchronises.
+static int display_impl(bh_ctx* ctx, const bh_display* d, int width, int height, uint8_t* out_rgb,
+                        double* exposure_used) {
+    if (!(d->glare >= 0.0 && d->glare <= 1.0)) return fail(ctx, BH_ERR_INVALID_ARG, "glare must be in [0, 1]");
+    if (d->tonemap < BH_TONEMAP_LINEAR || d->tonemap > BH_TONEMAP_HDR)
+        return fail(ctx, BH_ERR_INVALID_ARG, "unknown tonemap");
+    const size_t npx = static_cast<size_t>(width) * height;
+    int rc;
+    DisplayLaunch L;
+    std::memset(&L, 0, sizeof L);
+    L.pixels = static_cast<bh_xyz*>(ctx->pixels.p);
+    L.width = width;
+    L.height = height;
+    L.glare = d->glare;
+    L.glare_radius = d->glare_radius;
+    if (d->glare > 0.0 && d->glare_radius > 0.0) {
+        // img::add_glare's kernels (image.cpp:61-68), normalised on the host.
+        std::vector<double> w;
+        int r[2];
+        for (int j = 0; j < 2; ++j) {
+            const double sigma = (j == 0) ? d->glare_radius : d->glare_radius * 3.0;
+            r[j] = std::max(1, static_cast<int>(std::ceil(3.0 * sigma)));
+            std::vector<double> k(2 * r[j] + 1);
+            double sum = 0.0;
+            for (int i = -r[j]; i <= r[j]; ++i) {
+                k[i + r[j]] = std::exp(-0.5 * (i * i) / (sigma * sigma));
+                sum += k[i + r[j]];
+            }
+            for (double& v : k) v /= sum;
+            w.insert(w.end(), k.begin(), k.end());
+        }
+        if ((rc = ensure(ctx, ctx->disp_k, w.size() * sizeof(double))) != BH_OK) return rc;
+        for (DevBuf* b : {&ctx->disp_tmp, &ctx->disp_near, &ctx->disp_far})
+            if ((rc = ensure(ctx, *b, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+        CK(cudaMemcpyAsync(ctx->disp_k.p, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        ctx->h2d += static_cast<long long>(w.size() * sizeof(double));
+        L.k_near = static_cast<const double*>(ctx->disp_k.p);
+        L.k_far = L.k_near + (2 * r[0] + 1);
+        L.r_near = r[0];
+        L.r_far = r[1];
+        L.tmp = static_cast<bh_xyz*>(ctx->disp_tmp.p);
+        L.nearp = static_cast<bh_xyz*>(ctx->disp_near.p);
+        L.farp = static_cast<bh_xyz*>(ctx->disp_far.p);
+    }
+    if ((rc = ensure(ctx, ctx->disp_state, sizeof(ExposureState) + 2 * sizeof(double))) != BH_OK) return rc;
+    if (out_rgb && (rc = ensure(ctx, ctx->disp_rgb, npx * 3)) != BH_OK) return rc;
+    L.exposure = d->exposure;
+    L.key = d->key;
+    L.state = static_cast<ExposureState*>(ctx->disp_state.p);
+    L.exposure_out = reinterpret_cast<double*>(static_cast<unsigned char*>(ctx->disp_state.p) + sizeof(ExposureState));
+    L.reduce_blocks = ctx->sm_count * 4;
+    L.tonemap = d->tonemap;
+    L.log_k = std::pow(10.0, std::min(std::max(d->log_decades, 1.0), 20.0));
+    L.denom = std::log10(1.0 + L.log_k);
+    L.rgb = out_rgb ? static_cast<uint8_t*>(ctx->disp_rgb.p) : nullptr;
+    CK(launch_display(L, ctx->stream));
+    double e = 0.0;
+    CK(cudaMemcpyAsync(&e, L.exposure_out, sizeof e, cudaMemcpyDeviceToHost, ctx->stream));
+    if (out_rgb) CK(cudaMemcpyAsync(out_rgb, ctx->disp_rgb.p, npx * 3, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->d2h += static_cast<long long>(sizeof e + (out_rgb ? npx * 3 : 0));
+    if (exposure_used) *exposure_used = e;
+    return BH_OK;
+}
+
+void bh_display_default(bh_display* d) {
+    if (!d) return;
+    std::memset(d, 0, sizeof *d);
+    d->exposure = 0.0;
+    d->key = 1.0;
+    d->glare = 0.0;
+    d->glare_radius = 3.0;
+    d->log_decades = 16.0;
+    d->tonemap = BH_TONEMAP_HDR;
+}
+
+int bh_gpu_develop(bh_ctx* ctx, const bh_xyz* pixels, int width, int height, const bh_display* d,
+                   uint8_t* out_rgb, double* exposure_used) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!pixels || !d) return fail(ctx, BH_ERR_INVALID_ARG, "pixels and display settings must not be NULL");
+    if (width <= 0 || height <= 0) return fail(ctx, BH_ERR_INVALID_ARG, "width and height must be positive");
+    CK(cudaSetDevice(ctx->device));
+    ctx->h2d = 0;
+    ctx->d2h = 0;
+    const size_t npx = static_cast<size_t>(width) * height;
+    int rc;
+    if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+    CK(cudaMemcpyAsync(ctx->pixels.p, pixels, npx * sizeof(bh_xyz), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h2d += static_cast<long long>(npx * sizeof(bh_xyz));
+    return display_impl(ctx, d, width, height, out_rgb, exposure_used);
+}
+
+int bh_gpu_render_rgb(bh_ctx* ctx, const bh_render_config* cfg, const bh_display* d, uint8_t* out_rgb,
+                      double* exposure_used, bh_render_stats* stats) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!d) return fail(ctx, BH_ERR_INVALID_ARG, "display settings must not be NULL");
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    std::vector<FrameParams> frames;
+    int rc = prepare_frames(ctx, cfg, 1, frames);
+    if (rc != BH_OK) return rc;
+    const size_t npx = static_cast<size_t>(cfg->width) * cfg->height;
+    if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+    if ((rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true)) != BH_OK)
+        return rc;
+    if ((rc = display_impl(ctx, d, cfg->width, cfg->height, out_rgb, exposure_used)) != BH_OK) return rc;
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return finish(ctx, 1, stats, nullptr, true, secs);
 }
 
 int bh_gpu_adjoint(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out) {

@@ -66,6 +66,10 @@ def load_library():
             "bh_blackbody_table": (C.c_int, [P(C.c_double)]),
             "bh_gpu_fma_peak": (C.c_int, [C.c_int, C.c_int, P(C.c_double)]),
             "bh_gpu_trace_noalloc": (C.c_int, [C.c_int, cfg_p, C.c_void_p, C.c_void_p]),
+            "bh_display_default": (None, [P(abi.bh_display)]),
+            "bh_gpu_develop": (C.c_int, [ctx_p, P(abi.bh_xyz), C.c_int, C.c_int, P(abi.bh_display),
+                                         P(C.c_uint8), P(C.c_double)]),
+            "bh_gpu_render_rgb": (C.c_int, [ctx_p, cfg_p, P(abi.bh_display), P(C.c_uint8), P(C.c_double), st_p]),
             "bh_gpu_adjoint": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4)]),
             "bh_gpu_adjoint_rays": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4), P(C.c_double),
                                               P(C.c_double)]),
@@ -186,6 +190,46 @@ class Renderer:
                 stats.append(r)
         self._check(rc)
         return outs
+
+    # -- display transform -----------------------------------------------------------
+    def display_settings(self, **kw) -> abi.bh_display:
+        """bh_display with the reference CLI's defaults (HDR, metered exposure,
+        no glare, 16 decades), fields overridden by keyword."""
+        d = abi.bh_display()
+        self.lib.bh_display_default(C.byref(d))
+        for k, v in kw.items():
+            if k == "tonemap" and isinstance(v, str):
+                v = abi.TONEMAP_NAMES.index(v)
+            setattr(d, k, v)
+        return d
+
+    def develop(self, xyz, display=None, meter_only: bool = False, **kw):
+        """add_glare + auto_exposure + develop of a (H, W, 3) XYZ image on the
+        GPU: returns (rgb uint8 (H, W, 3) or None, exposure)."""
+        a = np.ascontiguousarray(xyz, dtype=np.float64)
+        h, w = a.shape[0], a.shape[1]
+        d = display if display is not None else self.display_settings(**kw)
+        out = None if meter_only else np.empty((h, w, 3), dtype=np.uint8)
+        e = C.c_double(0.0)
+        u8 = out.ctypes.data_as(C.POINTER(C.c_uint8)) if out is not None else None
+        self._check(self.lib.bh_gpu_develop(self._h, a.ctypes.data_as(C.POINTER(abi.bh_xyz)), w, h,
+                                            C.byref(d), u8, C.byref(e)))
+        return out, e.value
+
+    def render_rgb(self, cfg, display=None, stats: RenderStats | None = None, meter_only: bool = False, **kw):
+        """Render and develop on the device: returns (rgb uint8 (H, W, 3) or
+        None, exposure); only the 8-bit image crosses to the host."""
+        c = _as_c(cfg)
+        d = display if display is not None else self.display_settings(**kw)
+        out = None if meter_only else np.empty((c.height, c.width, 3), dtype=np.uint8)
+        e = C.c_double(0.0)
+        st = stats.to_c() if stats is not None else abi.bh_render_stats()
+        u8 = out.ctypes.data_as(C.POINTER(C.c_uint8)) if out is not None else None
+        rc = self.lib.bh_gpu_render_rgb(self._h, C.byref(c), C.byref(d), u8, C.byref(e), C.byref(st))
+        if stats is not None:
+            stats.update_from(st)
+        self._check(rc)
+        return out, e.value
 
     # -- discrete adjoint ----------------------------------------------------------
     def adjoint(self, cfg, target, per_ray: bool = False):

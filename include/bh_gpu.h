@@ -349,6 +349,43 @@ int  bh_gpu_adjoint(bh_ctx* ctx, const bh_render_config* cfg, const float* targe
 int  bh_gpu_adjoint_rays(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out,
                          double* ray_grad, double* ray_Y);
 
+/* Tone curves of the display transform, in img::ToneMap order (image.h:16). */
+enum {
+    BH_TONEMAP_LINEAR = 0,
+    BH_TONEMAP_REINHARD = 1,
+    BH_TONEMAP_ACES = 2,
+    BH_TONEMAP_LOG = 3,
+    BH_TONEMAP_HDR = 4
+};
+
+/* The display settings of the reference CLI (main.cpp:20-29, 905-909). */
+typedef struct bh_display {
+    double exposure;         /* > 0: this multiplier; <= 0: metered (img::auto_exposure) */
+    double key;              /* auto_exposure's key (1.0)                          */
+    double glare;            /* add_glare strength in [0, 1]; 0 = off (the default) */
+    double glare_radius;     /* add_glare radius in pixels (3.0)                   */
+    double log_decades;      /* decades of the Log and HDR curves (16.0)           */
+    int32_t tonemap;         /* BH_TONEMAP_* (BH_TONEMAP_HDR)                      */
+    int32_t reserved;
+} bh_display;
+
+void bh_display_default(bh_display* d);
+
+/* Replaces img::add_glare + img::auto_exposure + img::develop (image.cpp:22-191)
+   on a caller's frame: `pixels` (W*H bh_xyz, row-major, host) is glared (on a
+   device copy: the caller's buffer is not changed), metered unless
+   d->exposure > 0, and developed into out_rgb (W*H*3 bytes, host; may be NULL
+   to meter only).  *exposure_used (may be NULL) receives the multiplier. */
+int  bh_gpu_develop(bh_ctx* ctx, const bh_xyz* pixels, int width, int height, const bh_display* d,
+                    uint8_t* out_rgb, double* exposure_used);
+
+/* bh_gpu_render and the display transform in one call, the frame never
+   leaving the device as XYZ: the sequence of main.cpp:905-909 with 3 bytes per
+   pixel copied back instead of 24.  out_rgb may be NULL (meter only, as the
+   animation's probe frame, main.cpp:931-944). */
+int  bh_gpu_render_rgb(bh_ctx* ctx, const bh_render_config* cfg, const bh_display* d, uint8_t* out_rgb,
+                       double* exposure_used, bh_render_stats* stats);
+
 /* Measured FMA throughput of `device` in TFLOP/s (2 FLOP per FMA) for
    BH_PRECISION_FP64 (binary64) or BH_PRECISION_MIXED (binary32): the ALU
    roofline of the trace kernel.  Extension; no counterpart in the reference. */

@@ -78,6 +78,16 @@ def _declare(lib, prefix: str) -> None:
     fn("render", C.c_int, _CFG, C.POINTER(abi.bh_xyz), _ST)
     fn("render_rows", C.c_int, _CFG, C.POINTER(C.c_int), C.c_int, C.c_int,
        C.POINTER(abi.bh_xyz), _ST, _PD)
+    _PX = C.POINTER(abi.bh_xyz)
+    _U8 = C.POINTER(C.c_uint8)
+    if prefix == "orc_":
+        fn("auto_exposure", _D, _PX, C.c_long, _D)
+        fn("add_glare", None, _PX, C.c_int, C.c_int, _D, _D)
+        fn("develop", None, _PX, C.c_long, _D, C.c_int, _D, _U8)
+    else:
+        fn("auto_exposure", _D, _PX, C.c_int, C.c_int, _D)
+        fn("add_glare", None, _PX, C.c_int, C.c_int, _D, _D)
+        fn("develop", None, _PX, C.c_int, C.c_int, _D, C.c_int, _D, _U8)
     if prefix == "orc_":
         fn("star_catalogue", C.c_int, C.c_int, C.c_uint64, C.c_int, _PD)
         fn("sky_radiance", C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, _PD, C.c_int, _D, _PD)
@@ -245,6 +255,38 @@ class Port:
         if rc != 0:
             raise RuntimeError(f"{self.prefix}render_rows failed: {abi.STATUS_NAMES.get(rc, rc)}")
         return out, st, setup.value
+
+    # -- display transform (image.cpp:22-191) ------------------------------------
+    @staticmethod
+    def _img(xyz):
+        a = np.ascontiguousarray(xyz, dtype=np.float64)
+        if a.ndim != 3 or a.shape[2] != 3:
+            raise ValueError("image must be (height, width, 3)")
+        return a
+
+    def auto_exposure(self, xyz, key=1.0):
+        a = self._img(xyz)
+        px = a.ctypes.data_as(C.POINTER(abi.bh_xyz))
+        if self.prefix == "orc_":
+            return self._f("auto_exposure")(px, a.shape[0] * a.shape[1], key)
+        return self._f("auto_exposure")(px, a.shape[1], a.shape[0], key)
+
+    def add_glare(self, xyz, strength, radius_px):
+        """The glared copy of the image."""
+        a = self._img(xyz).copy()
+        self._f("add_glare")(a.ctypes.data_as(C.POINTER(abi.bh_xyz)), a.shape[1], a.shape[0], strength, radius_px)
+        return a
+
+    def develop(self, xyz, exposure, tonemap=abi.TONEMAP_HDR, log_decades=16.0):
+        a = self._img(xyz)
+        out = np.empty((a.shape[0], a.shape[1], 3), dtype=np.uint8)
+        px = a.ctypes.data_as(C.POINTER(abi.bh_xyz))
+        u8 = out.ctypes.data_as(C.POINTER(C.c_uint8))
+        if self.prefix == "orc_":
+            self._f("develop")(px, a.shape[0] * a.shape[1], exposure, tonemap, log_decades, u8)
+        else:
+            self._f("develop")(px, a.shape[1], a.shape[0], exposure, tonemap, log_decades, u8)
+        return out
 
     def scalar(self, name, *args):
         return self._f(name)(*args)

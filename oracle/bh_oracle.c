@@ -1286,3 +1286,161 @@ int orc_render_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                       bh_render_stats* stats) {
     return run_window(cfg, x0, y0, w, h, NULL, out, stats);
 }
+
+
+/* ---- display transform (image.cpp:22-191, spectrum.cpp:137-152) ------------ */
+
+static int cmp_double(const void* a, const void* b) {
+    const double x = *(const double*)a, y = *(const double*)b;
+    return (x > y) - (x < y);
+}
+
+/* image.cpp:22-45: the 99.9th and 99.99th percentiles (order statistics
+   k = (size_t)(q (n - 1)) of the positive finite luminances) set the
+   exposure.  A sort gives the same order statistic as nth_element. */
+double orc_auto_exposure(const bh_xyz* px, long n, double key) {
+    double* lum = (double*)malloc((size_t)(n > 0 ? n : 1) * sizeof(double));
+    size_t m = 0;
+    for (long i = 0; i < n; ++i)
+        if (px[i].y > 0.0 && isfinite(px[i].y)) lum[m++] = px[i].y;
+    if (m == 0) {
+        free(lum);
+        return 1.0;
+    }
+    qsort(lum, m, sizeof(double), cmp_double);
+    size_t k1 = (size_t)(0.999 * (double)(m - 1));
+    if (k1 > m - 1) k1 = m - 1;
+    size_t k2 = (size_t)(0.9999 * (double)(m - 1));
+    if (k2 > m - 1) k2 = m - 1;
+    const double hi = lum[k1], peak = lum[k2];
+    free(lum);
+    double e = 1.0;
+    if (hi > 0.0) e = key / hi;
+    if (peak > 0.0) {
+        const double c = 3.0 * key / peak;
+        if (c < e) e = c;
+    }
+    return e;
+}
+
+static int clampi(int v, int lo, int hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
+
+/* One separable Gaussian blur with clamped edges (image.cpp:60-91). */
+static void glare_blur(const bh_xyz* src, int w, int h, double sigma, bh_xyz* dst) {
+    int r = (int)ceil(3.0 * sigma);
+    if (r < 1) r = 1;
+    double* k = (double*)malloc((size_t)(2 * r + 1) * sizeof(double));
+    double sum = 0.0;
+    for (int i = -r; i <= r; ++i) {
+        k[i + r] = exp(-0.5 * (i * i) / (sigma * sigma));
+        sum += k[i + r];
+    }
+    for (int i = 0; i < 2 * r + 1; ++i) k[i] /= sum;
+    bh_xyz* tmp = (bh_xyz*)malloc((size_t)w * h * sizeof(bh_xyz));
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            bh_xyz a = {0.0, 0.0, 0.0};
+            for (int i = -r; i <= r; ++i) {
+                const bh_xyz* q = &src[(size_t)y * w + clampi(x + i, 0, w - 1)];
+                a.x += k[i + r] * q->x;
+                a.y += k[i + r] * q->y;
+                a.z += k[i + r] * q->z;
+            }
+            tmp[(size_t)y * w + x] = a;
+        }
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            bh_xyz a = {0.0, 0.0, 0.0};
+            for (int i = -r; i <= r; ++i) {
+                const bh_xyz* q = &tmp[(size_t)clampi(y + i, 0, h - 1) * w + x];
+                a.x += k[i + r] * q->x;
+                a.y += k[i + r] * q->y;
+                a.z += k[i + r] * q->z;
+            }
+            dst[(size_t)y * w + x] = a;
+        }
+    free(tmp);
+    free(k);
+}
+
+/* image.cpp:47-104: a narrow (radius) and a wide (3 radius) Gaussian. */
+void orc_add_glare(bh_xyz* px, int w, int h, double strength, double radius_px) {
+    if (strength <= 0.0 || radius_px <= 0.0) return;
+    const size_t n = (size_t)w * h;
+    bh_xyz* nearp = (bh_xyz*)malloc(n * sizeof(bh_xyz));
+    bh_xyz* farp = (bh_xyz*)malloc(n * sizeof(bh_xyz));
+    glare_blur(px, w, h, radius_px, nearp);
+    glare_blur(px, w, h, radius_px * 3.0, farp);
+    const double core = 1.0 - strength;
+    const double a = 0.7 * strength, b = 0.3 * strength;
+    for (size_t i = 0; i < n; ++i) {
+        px[i].x = px[i].x * core + nearp[i].x * a + farp[i].x * b;
+        px[i].y = px[i].y * core + nearp[i].y * a + farp[i].y * b;
+        px[i].z = px[i].z * core + nearp[i].z * a + farp[i].z * b;
+    }
+    free(nearp);
+    free(farp);
+}
+
+static double clampd_(double v, double lo, double hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
+
+static double aces_curve(double x) {   /* Narkowicz's ACES fit, image.cpp:106-110 */
+    const double a = 2.51, b = 0.03, c = 2.43, d = 0.59, e = 0.14;
+    return clampd_((x * (a * x + b)) / (x * (c * x + d) + e), 0.0, 1.0);
+}
+
+static double srgb_encode(double v) {  /* image.cpp:112-115 */
+    v = clampd_(v, 0.0, 1.0);
+    return (v <= 0.0031308) ? 12.92 * v : 1.055 * pow(v, 1.0 / 2.4) - 0.055;
+}
+
+/* image.cpp:117-191 with spectrum.cpp:137-152 (XYZ -> linear sRGB, gamut clamp). */
+void orc_develop(const bh_xyz* px, long n, double exposure, int tonemap, double log_decades,
+                 uint8_t* out) {
+    const double log_k = pow(10.0, clampd_(log_decades, 1.0, 20.0));
+    for (long i = 0; i < n; ++i) {
+        bh_xyz c = px[i];
+        if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) c.x = c.y = c.z = 0.0;
+        c.x *= exposure;
+        c.y *= exposure;
+        c.z *= exposure;
+        double v[3];
+        v[0] = 3.2404542 * c.x - 1.5371385 * c.y - 0.4985314 * c.z;
+        v[1] = -0.9692660 * c.x + 1.8760108 * c.y + 0.0415560 * c.z;
+        v[2] = 0.0556434 * c.x - 0.2040259 * c.y + 1.0572252 * c.z;
+        double m = v[0];
+        if (v[1] < m) m = v[1];
+        if (v[2] < m) m = v[2];
+        if (!(m >= 0.0)) {
+            v[0] -= m;
+            v[1] -= m;
+            v[2] -= m;
+        }
+        for (int ch = 0; ch < 3; ++ch)
+            if (v[ch] < 0.0) v[ch] = 0.0;
+        for (int ch = 0; ch < 3; ++ch) {
+            double x = v[ch];
+            switch (tonemap) {
+            case 0: x = clampd_(x, 0.0, 1.0); break;
+            case 1: x = x / (1.0 + x); break;
+            case 2: x = aces_curve(x); break;
+            case 3: {
+                const double denom = log10(1.0 + log_k);
+                x = clampd_(log10(1.0 + log_k * (x < 0.0 ? 0.0 : x)) / denom, 0.0, 1.0);
+                break;
+            }
+            default: {
+                const double cap = 0.12, wt = 0.5;
+                const double denom = log10(1.0 + log_k);
+                const double f = aces_curve(x);
+                const double l = clampd_(log10(1.0 + log_k * (x < 0.0 ? 0.0 : x)) / denom, 0.0, 1.0);
+                const double lift = cap * tanh(wt * l / cap);
+                x = clampd_(f + lift * (1.0 - f), 0.0, 1.0);
+                break;
+            }
+            }
+            v[ch] = x;
+        }
+        for (int ch = 0; ch < 3; ++ch) out[i * 3 + ch] = (uint8_t)lround(255.0 * srgb_encode(v[ch]));
+    }
+}

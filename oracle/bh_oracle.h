@@ -78,6 +78,13 @@ int    orc_trace_rays(const bh_render_config* cfg, int x0, int y0, int w, int h,
 int    orc_render_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                          bh_xyz* out, bh_render_stats* stats);
 
+/* Display transform (image.cpp:22-191).  tonemap: 0 Linear, 1 Reinhard,
+   2 ACES, 3 Log, 4 HDR (img::ToneMap order). */
+double orc_auto_exposure(const bh_xyz* px, long n, double key);
+void   orc_add_glare(bh_xyz* px, int w, int h, double strength, double radius_px);
+void   orc_develop(const bh_xyz* px, long n, double exposure, int tonemap, double log_decades,
+                   uint8_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,7 @@
 #define private public
 #include "render.cpp"
 #undef private
+#include "image.h"
 
 #include "../include/bh_gpu.h"
 
@@ -379,6 +380,30 @@ int ref_sky_radiance(int count, uint64_t seed, int milky_way, const double* dirs
         out3[3 * i] = c.x; out3[3 * i + 1] = c.y; out3[3 * i + 2] = c.z;
     }
     return BH_OK;
+}
+
+// The display transform (image.cpp:22-191), through the reference's own img::.
+namespace {
+img::Image to_image(const bh_xyz* px, int w, int h) {
+    img::Image im(w, h);
+    for (size_t i = 0; i < im.pixels.size(); ++i) im.pixels[i] = {px[i].x, px[i].y, px[i].z};
+    return im;
+}
+}  // namespace
+
+double ref_auto_exposure(const bh_xyz* px, int w, int h, double key) {
+    return img::auto_exposure(to_image(px, w, h), key);
+}
+void ref_add_glare(bh_xyz* px, int w, int h, double strength, double radius_px) {
+    img::Image im = to_image(px, w, h);
+    img::add_glare(im, strength, radius_px);
+    for (size_t i = 0; i < im.pixels.size(); ++i) px[i] = {im.pixels[i].x, im.pixels[i].y, im.pixels[i].z};
+}
+void ref_develop(const bh_xyz* px, int w, int h, double exposure, int tonemap, double log_decades,
+                 uint8_t* out) {
+    const std::vector<uint8_t> rgb =
+        img::develop(to_image(px, w, h), exposure, static_cast<img::ToneMap>(tonemap), log_decades);
+    std::memcpy(out, rgb.data(), rgb.size());
 }
 
 }  // extern "C"
