@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the 64-frame batch leg")
     p.add_argument("--no-photon-ring", action="store_true", help="skip the 4096^2 photon-ring leg")
     p.add_argument("--no-adjoint", action="store_true", help="skip the 512^2 adjoint leg")
+    p.add_argument("--no-display", action="store_true", help="skip the on-device display leg")
     p.add_argument("--once", action="store_true",
                    help="render the frame once in mixed precision and once in FP64 and exit (for ncu captures)")
     return p.parse_args()
@@ -451,6 +452,27 @@ def gpu_arm(args):
     out["e2e"] = {"value": round(world * rays * args.steps / t_e2e, 1), "unit": "rays/s",
                   "h2d_bytes_per_step": int(st_e.h2d_bytes), "d2h_bytes_per_step": int(st_e.d2h_bytes),
                   "api": "bh_gpu_render (C-ABI) into pinned host memory, wall clock"}
+
+    # Display leg: the same frame developed on the device (HDR curve, metered
+    # exposure) so that only 8-bit sRGB crosses to the host.
+    if not args.no_display:
+        try:
+            for _ in range(max(1, args.warmup)):
+                r.render_rgb(cfg_m)
+            barrier()
+            t0 = time.perf_counter()
+            st_d = RenderStats()
+            for _ in range(args.steps):
+                st_d = RenderStats()
+                rgb, e = r.render_rgb(cfg_m, stats=st_d)
+            t_rgb = max_over_ranks(time.perf_counter() - t0)
+            barrier()
+            out["display"] = {"value": round(world * rays * args.steps / t_rgb, 1), "unit": "rays/s",
+                              "api": "bh_gpu_render_rgb (render + auto exposure + HDR tone curve + sRGB on "
+                                     "the device), 8-bit image into host memory, wall clock",
+                              "d2h_bytes_per_step": int(st_d.d2h_bytes), "exposure": e}
+        except Exception as e:  # reported, not hidden
+            out["display"] = {"error": repr(e)}
 
     # Kernels of ours launched in the timed region per mixed step: trace,
     # binary64 resume trace, shade, 2 reduce.
