@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # Status codes (bh_gpu.h).
 OK = 0
@@ -80,6 +80,15 @@ class bh_neutron_star(C.Structure):
     ]
 
 
+JET_PARAMS = ("z_base", "z_top", "R_base", "k", "gamma_max", "z_sat", "alpha", "u_peak", "u_wid", "spine",
+              "spine_wid", "zeta", "eps_rad", "phi_flux")
+JET_CONFIGURED = ("a", "Omega_F", "P_jet", "L_rad", "j_nu0", "r_bound", "volume_rg3")
+
+
+class bh_jet(C.Structure):
+    _fields_ = [(k, C.c_double) for k in JET_PARAMS + JET_CONFIGURED]
+
+
 class bh_render_config(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("abi_version", C.c_uint32),
@@ -103,6 +112,7 @@ class bh_render_config(C.Structure):
         ("milky_way", C.c_int32),
         ("stop_epsilon", C.c_double),
         ("mixed_rtol", C.c_double), ("mixed_atol", C.c_double),
+        ("jet", bh_jet),
     ]
 
 
@@ -128,6 +138,7 @@ class bh_ray_result(C.Structure):
         ("xyz", bh_xyz),
         ("attempts", C.c_int32), ("reserved", C.c_int32),
         ("max_norm", C.c_double), ("max_q", C.c_double),
+        ("jet", C.c_double),
     ]
 
 
@@ -204,10 +215,10 @@ def ray_result_dtype():
 
     return np.dtype(
         {
-            "names": ["what", "steps", "y", "g", "dir", "xyz", "attempts", "max_norm", "max_q"],
+            "names": ["what", "steps", "y", "g", "dir", "xyz", "attempts", "max_norm", "max_q", "jet"],
             "formats": [np.int32, np.int32, (np.float64, 8), np.float64, (np.float64, 3), (np.float64, 3),
-                        np.int32, np.float64, np.float64],
-            "offsets": [0, 4, 8, 72, 80, 104, 128, 136, 144],
+                        np.int32, np.float64, np.float64, np.float64],
+            "offsets": [0, 4, 8, 72, 80, 104, 128, 136, 144, 152],
             "itemsize": C.sizeof(bh_ray_result),
         }
     )

@@ -79,6 +79,45 @@ class NeutronStar:
 
 
 @dataclass
+class Jet:
+    """bh::Jet (jet.h:96-146) without `enabled` (RenderConfig.jet_enabled).
+    The last block is what Jet::configure sets (``configure`` below, or
+    ``RenderConfig.setup_jet()`` for the CLI's set-up)."""
+
+    z_base: float = 3.0
+    z_top: float = 120.0
+    R_base: float = 1.6
+    k: float = 0.58
+    gamma_max: float = 10.0
+    z_sat: float = 80.0
+    alpha: float = 0.7
+    u_peak: float = 0.82
+    u_wid: float = 0.17
+    spine: float = 0.06
+    spine_wid: float = 0.40
+    zeta: float = 2.0
+    eps_rad: float = 0.02
+    phi_flux: float = 50.0
+    a: float = 0.0
+    Omega_F: float = 0.0
+    P_jet: float = 0.0
+    L_rad: float = 0.0
+    j_nu0: float = 0.0
+    r_bound: float = 0.0
+    volume_rg3: float = 0.0
+
+    def to_c(self) -> abi.bh_jet:
+        j = abi.bh_jet()
+        for k in abi.JET_PARAMS + abi.JET_CONFIGURED:
+            setattr(j, k, float(getattr(self, k)))
+        return j
+
+    def update_from(self, j: abi.bh_jet) -> None:
+        for k in abi.JET_PARAMS + abi.JET_CONFIGURED:
+            setattr(self, k, getattr(j, k))
+
+
+@dataclass
 class RenderConfig:
     """bh::RenderConfig (render.h:15-53) plus the GPU extensions.
 
@@ -109,6 +148,7 @@ class RenderConfig:
     hotspot: HotSpot = field(default_factory=HotSpot)
     star: NeutronStar = field(default_factory=NeutronStar)
     jet_enabled: bool = False
+    jet: Jet = field(default_factory=Jet)
     observer_time: float = 0.0
     rtol: float = 1e-9
     atol: float = 1e-11
@@ -176,7 +216,22 @@ class RenderConfig:
         c.stop_epsilon = self.stop_epsilon
         c.mixed_rtol = self.mixed_rtol
         c.mixed_atol = self.mixed_atol
+        c.jet = self.jet.to_c()
         return c
+
+    def setup_jet(self) -> "RenderConfig":
+        """The CLI's jet set-up (main.cpp:399-423) through the library:
+        configures ``jet`` from the disc's accretion rate, or switches the
+        jet off where the reference does.  Returns self."""
+        from .gpu import load_library
+
+        c = self.to_c()
+        rc = load_library().bh_render_config_setup_jet(C.byref(c))
+        if rc != abi.OK:
+            raise ValueError(f"bh_render_config_setup_jet failed ({rc})")
+        self.jet_enabled = bool(c.jet_enabled)
+        self.jet.update_from(c.jet)
+        return self
 
     def replace(self, **kw) -> "RenderConfig":
         import copy

@@ -59,7 +59,7 @@ struct bh_ctx {
     int32_t* d_bin_start = nullptr;
     HostSky sky_meta;
 
-    DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats, deferred;
+    DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats, deferred, jet;
     // Adjoint: target image, per-ray gradients and luminances, checkpoint
     // slots, counters and the five sums.
     DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums;
@@ -194,6 +194,7 @@ void stats_add(bh_render_stats* s, const FrameStats& f) {
     s->star_hits += (long long)f.star_hits;
     s->escaped += (long long)f.escaped;
     s->exhausted += (long long)f.exhausted;
+    s->jet_rays += (long long)f.jet_rays;
     double mn, mq;
     std::memcpy(&mn, &f.max_norm_bits, sizeof mn);
     std::memcpy(&mq, &f.max_q_bits, sizeof mq);
@@ -239,6 +240,9 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
         return rc;
     if ((rc = ensure(ctx, ctx->fstats, n * sizeof(FrameStats))) != BH_OK) return rc;
     p.mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
+    bool any_jet = false;
+    for (int i = 0; i < n; ++i) any_jet = any_jet || frames[i].jet_enabled;
+    if (any_jet && (rc = ensure(ctx, ctx->jet, static_cast<size_t>(rays) * sizeof(double))) != BH_OK) return rc;
     if (p.mixed && (rc = ensure(ctx, ctx->deferred, static_cast<size_t>(rays) * deferred_record_bytes())) != BH_OK)
         return rc;
 
@@ -296,6 +300,7 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
         tl.grid_resume = ctx->sm_count * (bps64 < 1 ? 1 : bps64);
     }
     tl.resume_event = timed ? ctx->ev[3] : nullptr;
+    tl.jet = any_jet ? static_cast<double*>(ctx->jet.p) : nullptr;
 
     ShadeLaunch& sl = p.sl;
     std::memset(&sl, 0, sizeof sl);
@@ -309,6 +314,7 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     sl.rays = d_rays;
     sl.pixel_lum = static_cast<double*>(ctx->lum.p);
     sl.ray_class = nullptr;
+    sl.jet = tl.jet;
 
     ReduceLaunch& rl = p.rl;
     std::memset(&rl, 0, sizeof rl);
@@ -316,6 +322,7 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     rl.nframes = n;
     rl.hits = tl.hits;
     rl.pixel_lum = sl.pixel_lum;
+    rl.jet = tl.jet;
     rl.partials = static_cast<FrameStats*>(ctx->partials.p);
     rl.out = static_cast<FrameStats*>(ctx->fstats.p);
     rl.blocks_per_frame = kReduceBlocks;
@@ -466,7 +473,7 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end, &ctx->deferred,
-                      &ctx->pix_end, &ctx->partials, &ctx->fstats, &ctx->adj_target, &ctx->adj_grad, &ctx->adj_Y,
+                      &ctx->pix_end, &ctx->partials, &ctx->fstats, &ctx->jet, &ctx->adj_target, &ctx->adj_grad, &ctx->adj_Y,
                       &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums, &ctx->disp_tmp, &ctx->disp_near,
                       &ctx->disp_far, &ctx->disp_k, &ctx->disp_state, &ctx->disp_rgb})
         if (b->p) cudaFree(b->p);
@@ -787,6 +794,15 @@ static int display_impl(bh_ctx* ctx, const bh_display* d, int width, int height,
     ctx->d2h += static_cast<long long>(sizeof e + (out_rgb ? npx * 3 : 0));
     if (exposure_used) *exposure_used = e;
     return BH_OK;
+}
+
+void bh_jet_configure(bh_jet* jet, double spin, double mdot_c2, double r_g_m) {
+    if (jet) jet_configure(*jet, spin, mdot_c2, r_g_m);
+}
+
+int bh_render_config_setup_jet(bh_render_config* cfg) {
+    if (!cfg) return BH_ERR_INVALID_ARG;
+    return setup_jet(*cfg);
 }
 
 void bh_display_default(bh_display* d) {

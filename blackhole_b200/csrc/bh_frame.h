@@ -78,6 +78,14 @@ struct FrameParams {
     double observer_time;
     int32_t precision_tag;           // BH_PRECISION_* of the launch
     int32_t pad3;
+
+    // ---- jet (jet.h:96-315; sampled per step, render.cpp:107-122) ------------
+    int32_t jet_enabled;
+    int32_t pad4;
+    double jet_z_base, jet_z_top, jet_R_base, jet_k, jet_gamma_max, jet_z_sat;
+    double jet_alpha, jet_u_peak, jet_u_wid, jet_spine, jet_spine_wid, jet_zeta;
+    double jet_Omega_F, jet_j_nu0, jet_r_bound;
+    double jet_col[3];               // powerlaw_xyz(alpha) (spectrum.cpp:77-92)
 };
 
 // Read-only sky data shared by all frames of a launch.
@@ -106,7 +114,7 @@ struct HitRecord {
 // Per-frame reduction target (device side), reduced into bh_render_stats.
 struct FrameStats {
     unsigned long long rays, steps, attempts;
-    unsigned long long captured, disc_hits, sun_hits, star_hits, escaped, exhausted;
+    unsigned long long captured, disc_hits, sun_hits, star_hits, escaped, exhausted, jet_rays;
     unsigned long long max_norm_bits, max_q_bits;   // non-negative doubles as ordered bits
     double total_flux;
 };

@@ -1,4 +1,4 @@
-// bh_launch.h - Host-side launch wrappers of the device kernels (bh_kernels.cu).
+// bh_launch.h - Host-side launch wrappers of the trace, shade and stats kernels.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,6 +29,8 @@ struct TraceLaunch {
     int block_resume;                // its threads per block
     int reg_variant_resume;          // its register cap (0 tight, 1 wide)
     cudaEvent_t resume_event;        // recorded between the two launches (optional)
+    double* jet;                     // jet emission per ray (total_rays), or null when no
+                                     // frame of the launch has a jet
 };
 
 // Bytes of one deferred-ray record.
@@ -54,6 +56,7 @@ struct ShadeLaunch {
     bh_ray_result* rays;             // optional device per-sample results (single frame)
     double* pixel_lum;               // device, total_pixels luminance for the flux sum
     unsigned char* ray_class;        // device, per-ray class after shading
+    const double* jet;               // jet emission per ray (TraceLaunch::jet), or null
 };
 
 cudaError_t launch_shade(const ShadeLaunch& L, cudaStream_t stream);
@@ -63,6 +66,7 @@ struct ReduceLaunch {
     int nframes;
     const HitRecord* hits;
     const double* pixel_lum;
+    const double* jet;               // jet emission per ray, or null
     FrameStats* partials;            // nframes * blocks_per_frame
     FrameStats* out;                 // nframes
     int blocks_per_frame;

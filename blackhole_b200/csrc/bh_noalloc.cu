@@ -82,6 +82,7 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
     int rc = make_frame(*cfg, F, err);
     if (rc != BH_OK) return rc;
     if (F.n_rays > BH_NOALLOC_MAX_RAYS) return BH_ERR_INVALID_ARG;
+    if (F.jet_enabled) return BH_ERR_UNSUPPORTED;   // the jet's per-ray sum has no slot here
     F.precision_tag = cfg->precision;
     F.ray_begin = 0;
     F.pixel_begin = 0;

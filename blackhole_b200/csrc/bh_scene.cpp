@@ -104,6 +104,39 @@ double bv_to_temperature(double bv) {  // spectrum.cpp:158-162 (Ballesteros 2012
     return 4600.0 * (1.0 / (0.92 * x + 1.7) + 1.0 / (0.92 * x + 0.62));
 }
 
+// spectrum.cpp:77-92: CIE colour of a unit power law I_nu ~ nu^-alpha.
+void powerlaw_xyz(double alpha, double out[3]) {
+    constexpr double lambda_0 = 550e-9;
+    out[0] = out[1] = out[2] = 0.0;
+    constexpr double lo = 360.0, hi = 830.0, dl = 1.0;
+    for (double nm = lo; nm <= hi; nm += dl) {
+        const double lam = nm * 1e-9;
+        const double I_l = kC * std::pow(lam / lambda_0, alpha) / (lam * lam);
+        const double w = I_l * dl * 1e-9;
+        out[0] += w * cie_x(nm);
+        out[1] += w * cie_y(nm);
+        out[2] += w * cie_z(nm);
+    }
+}
+
+// ---- jet.h:77-315 (the host half: power and emissivity normalisation) ---------
+double smoothstep01(double t) {
+    t = clampd(t, 0.0, 1.0);
+    return t * t * (3.0 - 2.0 * t);
+}
+double jet_radius(const bh_jet& j, double z_abs) {
+    return j.R_base * std::pow(maxd(z_abs, 1e-6) / j.z_base, j.k);
+}
+double jet_gamma_at(const bh_jet& j, double z_abs) {
+    const double t = std::min(1.0, std::pow(maxd(z_abs, 1e-6) / j.z_sat, j.k));
+    return 1.0 + (j.gamma_max - 1.0) * t;
+}
+double jet_radial_profile(const bh_jet& j, double u) {
+    const double s = (u - j.u_peak) / j.u_wid;
+    const double t = u / j.spine_wid;
+    return std::exp(-s * s) + j.spine * std::exp(-t * t);
+}
+
 // ---- scene.h:27-44 -------------------------------------------------------------
 struct Rng {
     uint64_t s;
@@ -259,7 +292,6 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     if (c.width > (1 << 16) || c.height > (1 << 16)) { err = "width/height above 65536"; return BH_ERR_INVALID_ARG; }
     const int S = std::max(1, c.sqrt_spp);
     if (S > 64) { err = "sqrt_spp above 64"; return BH_ERR_INVALID_ARG; }
-    if (c.jet_enabled) { err = "jets are not built in the GPU path"; return BH_ERR_UNSUPPORTED; }
     if (c.precision != BH_PRECISION_FP64 && c.precision != BH_PRECISION_MIXED) {
         err = "unknown precision";
         return BH_ERR_INVALID_ARG;
@@ -415,6 +447,103 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     F.hs_contrast = c.hotspot.contrast;
     F.hs_omega = c.hotspot.omega;
     F.observer_time = c.observer_time;
+
+    // Jet: the model as configured (render() reads cfg.jet as given).
+    F.jet_enabled = c.jet_enabled ? 1 : 0;
+    if (c.jet_enabled) {
+        const bh_jet& j = c.jet;
+        if (!(j.z_base > 0.0) || !(j.z_sat > 0.0) || !(j.R_base > 0.0) || !(j.u_wid > 0.0) ||
+            !(j.spine_wid > 0.0) || !(j.z_top > 0.0)) {
+            err = "jet z_base, z_top, z_sat, R_base, u_wid and spine_wid must be positive";
+            return BH_ERR_INVALID_ARG;
+        }
+        F.jet_z_base = j.z_base;
+        F.jet_z_top = j.z_top;
+        F.jet_R_base = j.R_base;
+        F.jet_k = j.k;
+        F.jet_gamma_max = j.gamma_max;
+        F.jet_z_sat = j.z_sat;
+        F.jet_alpha = j.alpha;
+        F.jet_u_peak = j.u_peak;
+        F.jet_u_wid = j.u_wid;
+        F.jet_spine = j.spine;
+        F.jet_spine_wid = j.spine_wid;
+        F.jet_zeta = j.zeta;
+        F.jet_Omega_F = j.Omega_F;
+        F.jet_j_nu0 = j.j_nu0;
+        F.jet_r_bound = j.r_bound;
+        powerlaw_xyz(j.alpha, F.jet_col);   // render.cpp:417
+    }
+    return BH_OK;
+}
+
+void jet_configure(bh_jet& j, double spin, double mdot_c2, double r_g_m) {
+    // kerr.h:204-207 and jet.h:81-87
+    const double rp = horizon_outer(spin);
+    const double OmH = (rp > 0.0) ? spin / (2.0 * rp) : 0.0;
+    j.a = spin;
+    j.Omega_F = 0.5 * OmH;
+    {
+        const double x = OmH * OmH;
+        const double f = 1.0 + 1.38 * x - 9.2 * x * x;
+        const double kappa = 0.053, phi = j.phi_flux;
+        j.P_jet = (kappa / (4.0 * kPi)) * phi * phi * x * std::max(0.0, f) * mdot_c2;
+    }
+    j.L_rad = j.eps_rad * j.P_jet;
+    j.r_bound = std::sqrt(j.z_top * j.z_top + jet_radius(j, j.z_top) * jet_radius(j, j.z_top)) * 1.05;
+    double C_f = 0.0;
+    {
+        constexpr int N = 2000;
+        const double du = 3.0 / N;
+        for (int i = 0; i < N; ++i) {
+            const double u = (i + 0.5) * du;
+            C_f += jet_radial_profile(j, u) * u * du;
+        }
+    }
+    double V = 0.0;
+    {
+        constexpr int N = 4000;
+        const double dz = (j.z_top - j.z_base) / N;
+        for (int i = 0; i < N; ++i) {
+            const double z = j.z_base + (i + 0.5) * dz;
+            const double R = jet_radius(j, z);
+            const double gz = std::pow(jet_gamma_at(j, z) / jet_gamma_at(j, j.z_base), -(2.0 + j.alpha)) *
+                              std::pow(R / j.R_base, -(3.0 + j.alpha)) * std::pow(z / j.z_base, j.zeta);
+            const double ramp = smoothstep01((z - j.z_base) / (0.5 * j.z_base)) *
+                                smoothstep01((j.z_top - z) / (0.15 * j.z_top));
+            V += gz * ramp * R * R * dz;
+        }
+        V *= 2.0 * (2.0 * kPi) * C_f;
+    }
+    j.volume_rg3 = V;
+    const double V_m3 = V * r_g_m * r_g_m * r_g_m;
+    if (!(V_m3 > 0.0) || !(j.L_rad > 0.0)) {
+        j.j_nu0 = 0.0;
+        return;
+    }
+    const double A = j.L_rad / (4.0 * kPi * V_m3);
+    constexpr double nu_0 = kC / 550e-9, nu_lo = 1.0e9, nu_hi = 1.0e17;
+    const double p = 1.0 - j.alpha;
+    const double band = (std::fabs(p) > 1e-9) ? (std::pow(nu_hi, p) - std::pow(nu_lo, p)) / p
+                                              : std::log(nu_hi / nu_lo);
+    j.j_nu0 = A / (std::pow(nu_0, j.alpha) * band) * r_g_m;
+}
+
+int setup_jet(bh_render_config& c) {
+    if (!c.jet_enabled) return BH_OK;
+    if (c.star.enabled || !c.disc_enabled) {   // no horizon, or no accretion flow
+        c.jet_enabled = 0;
+        return BH_OK;
+    }
+    c.jet.z_sat = std::min(c.jet.z_sat, 0.7 * c.jet.z_top);
+    const double ad = clampd(c.spin, -0.9999, 0.9999);
+    const int sg = c.disc_sense;
+    const double eta = 1.0 - circular_energy(ad, isco_radius(ad, sg), sg);
+    const double L_edd = 4.0 * kPi * kG * c.M_kg * kMp * kC / kSigmaT;
+    const double mdot = c.eddington * (L_edd / (eta * kC * kC));
+    const double r_g = kG * c.M_kg / (kC * kC);
+    jet_configure(c.jet, c.spin, mdot * kC * kC, r_g);
+    if (!(c.jet.P_jet > 0.0)) c.jet_enabled = 0;
     return BH_OK;
 }
 
@@ -460,6 +589,21 @@ void default_config(bh_render_config& c) {
     c.sky_mode = BH_SKY_GALACTIC;
     c.stop_mode = BH_STOP_REFERENCE;
     c.milky_way = 1;
+    // jet.h:96-146
+    c.jet.z_base = 3.0;
+    c.jet.z_top = 120.0;
+    c.jet.R_base = 1.6;
+    c.jet.k = 0.58;
+    c.jet.gamma_max = 10.0;
+    c.jet.z_sat = 80.0;
+    c.jet.alpha = 0.7;
+    c.jet.u_peak = 0.82;
+    c.jet.u_wid = 0.17;
+    c.jet.spine = 0.06;
+    c.jet.spine_wid = 0.40;
+    c.jet.zeta = 2.0;
+    c.jet.eps_rad = 0.02;
+    c.jet.phi_flux = 50.0;
 }
 
 }  // namespace bhg

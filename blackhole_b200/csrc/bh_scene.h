@@ -41,7 +41,12 @@ int star_catalogue(int count, uint64_t seed, int sky_mode, double* out6);
 // Validate a config and fill the frame constants.  Returns a bh_status.
 int make_frame(const bh_render_config& c, FrameParams& F, std::string& err);
 
-// The reference defaults (render.h:15-53, scene.h:232-351, neutronstar.h:43-70).
+// The reference defaults (render.h:15-53, scene.h:232-351, neutronstar.h:43-70,
+// jet.h:96-146).
 void default_config(bh_render_config& c);
+
+// Jet::configure (jet.h:262-312) and the CLI's jet set-up (main.cpp:399-423).
+void jet_configure(bh_jet& j, double spin, double mdot_c2, double r_g_m);
+int setup_jet(bh_render_config& c);
 
 }  // namespace bhg

@@ -293,6 +293,7 @@ struct ShadeArgs {
     bh_xyz* pixels;
     bh_ray_result* rays;
     double* pixel_lum;
+    const double* jet;
 };
 
 __global__ void shade_kernel(ShadeArgs A) {
@@ -310,6 +311,14 @@ __global__ void shade_kernel(ShadeArgs A) {
         const HitRecord hr = A.hits[rid];
         double c[3], g, dir[3];
         shade_one(A.sky, F, hr, c, &g, dir);
+        // Whatever the ray ended on, the jet light it collected on the way is
+        // added in the jet's one colour (render.cpp:377-392).
+        const double jet = (F.jet_enabled && A.jet) ? A.jet[rid] : 0.0;
+        if (jet > 0.0) {
+            c[0] += F.jet_col[0] * jet;
+            c[1] += F.jet_col[1] * jet;
+            c[2] += F.jet_col[2] * jet;
+        }
         acc[0] += c[0]; acc[1] += c[1]; acc[2] += c[2];
         if (A.rays) {
             bh_ray_result& o = A.rays[((long long)py * F.width + px) * SS + k];
@@ -324,6 +333,7 @@ __global__ void shade_kernel(ShadeArgs A) {
             o.reserved = 0;
             o.max_norm = hr.max_norm;
             o.max_q = hr.max_q;
+            o.jet = jet;
         }
     }
     const double w = F.inv_SS;
@@ -341,6 +351,7 @@ struct ReduceArgs {
     int nframes;
     const HitRecord* hits;
     const double* pixel_lum;
+    const double* jet;
     FrameStats* partials;
     FrameStats* out;
     int bpf;
@@ -353,10 +364,11 @@ constexpr int kRedThreads = 256;
 __global__ void __launch_bounds__(kRedThreads) reduce_partial_kernel(ReduceArgs A) {
     const int f = blockIdx.y;
     const FrameParams& F = A.frames[f];
-    __shared__ unsigned long long s_cnt[kRedThreads][9];
+    __shared__ unsigned long long s_cnt[kRedThreads][10];
     __shared__ double s_max[kRedThreads][2];
     __shared__ double s_flux[kRedThreads];
-    unsigned long long c[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long c[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double* jet = (F.jet_enabled && A.jet) ? A.jet + F.ray_begin : nullptr;
     double mn = 0.0, mq = 0.0, flux = 0.0;
     const long long stride = (long long)A.bpf * kRedThreads;
     for (long long i = (long long)blockIdx.x * kRedThreads + threadIdx.x; i < F.n_rays; i += stride) {
@@ -367,18 +379,19 @@ __global__ void __launch_bounds__(kRedThreads) reduce_partial_kernel(ReduceArgs 
         if (h.what >= 0 && h.what <= 5) c[3 + h.what] += 1;
         mn = dmaxr(mn, h.max_norm);
         mq = dmaxr(mq, h.max_q);
+        if (jet && jet[i] > 0.0) c[9] += 1;
     }
     const long long npx = (long long)F.width * F.height;
     for (long long i = (long long)blockIdx.x * kRedThreads + threadIdx.x; i < npx; i += stride)
         flux += A.pixel_lum[F.pixel_begin + i];
-    for (int k = 0; k < 9; ++k) s_cnt[threadIdx.x][k] = c[k];
+    for (int k = 0; k < 10; ++k) s_cnt[threadIdx.x][k] = c[k];
     s_max[threadIdx.x][0] = mn;
     s_max[threadIdx.x][1] = mq;
     s_flux[threadIdx.x] = flux;
     __syncthreads();
     for (int off = kRedThreads / 2; off > 0; off >>= 1) {
         if (threadIdx.x < off) {
-            for (int k = 0; k < 9; ++k) s_cnt[threadIdx.x][k] += s_cnt[threadIdx.x + off][k];
+            for (int k = 0; k < 10; ++k) s_cnt[threadIdx.x][k] += s_cnt[threadIdx.x + off][k];
             s_max[threadIdx.x][0] = dmaxr(s_max[threadIdx.x][0], s_max[threadIdx.x + off][0]);
             s_max[threadIdx.x][1] = dmaxr(s_max[threadIdx.x][1], s_max[threadIdx.x + off][1]);
             s_flux[threadIdx.x] += s_flux[threadIdx.x + off];
@@ -396,6 +409,7 @@ __global__ void __launch_bounds__(kRedThreads) reduce_partial_kernel(ReduceArgs 
         o.star_hits = s_cnt[0][3 + BH_HIT_STAR];
         o.escaped = s_cnt[0][3 + BH_HIT_SKY];
         o.exhausted = s_cnt[0][3 + BH_HIT_EXHAUSTED];
+        o.jet_rays = s_cnt[0][9];
         o.max_norm_bits = dbits(s_max[0][0]);
         o.max_q_bits = dbits(s_max[0][1]);
         o.total_flux = s_flux[0];
@@ -412,6 +426,7 @@ __global__ void reduce_final_kernel(ReduceArgs A) {
         t.rays += p.rays; t.steps += p.steps; t.attempts += p.attempts;
         t.captured += p.captured; t.disc_hits += p.disc_hits; t.sun_hits += p.sun_hits;
         t.star_hits += p.star_hits; t.escaped += p.escaped; t.exhausted += p.exhausted;
+        t.jet_rays += p.jet_rays;
         mn = dmaxr(mn, __longlong_as_double((long long)p.max_norm_bits));
         mq = dmaxr(mq, __longlong_as_double((long long)p.max_q_bits));
         t.total_flux += p.total_flux;
@@ -436,6 +451,7 @@ cudaError_t launch_shade(const ShadeLaunch& L, cudaStream_t stream) {
     A.pixels = L.pixels;
     A.rays = L.rays;
     A.pixel_lum = L.pixel_lum;
+    A.jet = L.jet;
     const int bs = 128;
     const long long grid = (L.total_pixels + bs - 1) / bs;
     shade_kernel<<<(unsigned)grid, bs, 0, stream>>>(A);
@@ -448,6 +464,7 @@ cudaError_t launch_reduce(const ReduceLaunch& L, cudaStream_t stream) {
     A.nframes = L.nframes;
     A.hits = L.hits;
     A.pixel_lum = L.pixel_lum;
+    A.jet = L.jet;
     A.partials = L.partials;
     A.out = L.out;
     A.bpf = L.blocks_per_frame;

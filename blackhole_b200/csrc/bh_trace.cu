@@ -26,6 +26,7 @@
 #include "bh_common.cuh"
 #include "bh_dp5.cuh"
 #include "bh_frame.h"
+#include "bh_jet.cuh"
 #include "bh_launch.h"
 
 namespace bhg {
@@ -135,6 +136,7 @@ struct Lane {
     float inv_Q0, max_norm, max_q;
     int steps, tries, attempts;
     int att0;                // attempts already counted against the budget
+    double jet;              // jet emission picked up so far (jet kernels only)
     int gid, frame;
     int have_k1;
     int factored;
@@ -264,6 +266,7 @@ struct TraceArgs {
     int rays_per_thread;
     int refill;
     unsigned long long budget;
+    double* jet;             // jet emission per ray (jet kernels only)
 };
 
 template <class P>
@@ -278,8 +281,9 @@ __device__ __forceinline__ void state8(const Lane<P>& L, const double ptph[2], d
     y8[7] = ptph[1];
 }
 
-template <class P>
+template <class P, bool JET>
 __device__ __forceinline__ void write_hit(const TraceArgs& A, const Lane<P>& L, int what, const double y8[8]) {
+    if (JET) A.jet[L.gid] = L.jet;
     // y[4] = p_t and y[7] = p_phi were stored exactly when the ray started.
     HitRecord* o = &A.hits[L.gid];
     o->y[0] = y8[0];
@@ -296,7 +300,7 @@ __device__ __forceinline__ void write_hit(const TraceArgs& A, const Lane<P>& L, 
 }
 
 // Lane set-up from an initial photon (fresh ray) or a deferred state.
-template <class P>
+template <class P, bool JET>
 __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     using R = typename P::R;
     const Deferred* dr = nullptr;
@@ -328,6 +332,7 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     L.bad_sc = (F.atol + F.rtol * fabs(y8[4]) == 0.0) || (F.atol + F.rtol * fabs(y8[7]) == 0.0);
     L.tries = 0;
     L.have_k1 = 0;
+    if (JET) L.jet = A.resume ? A.jet[L.gid] : 0.0;
     // p_t and p_phi never change: store them now, the rest at termination.
     A.hits[L.gid].y[4] = y8[4];
     A.hits[L.gid].y[7] = y8[7];
@@ -365,7 +370,7 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     L.errp_pow = (R)P::powd(dmaxr((double)L.err_prev, 1e-4), kBeta);
     L.inv_Q0 = (float)(1.0 / (fabs(L.Q0) + 1e-12));
     if (!dr && F.max_steps <= 0) {
-        write_hit(A, L, BH_HIT_EXHAUSTED, y8);
+        write_hit<P, JET>(A, L, BH_HIT_EXHAUSTED, y8);
         return false;
     }
     return true;
@@ -373,7 +378,7 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
 
 // One step attempt.  Returns true when the lane's ray is finished here
 // (terminated, or deferred to the binary64 kernel).
-template <class P>
+template <class P, bool JET>
 __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     using R = typename P::R;
     const FrameParams& F = A.frames[L.frame];
@@ -452,7 +457,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             // with the ray's initial state.
             double y8[8], Q0;
             ray_setup(F, (long long)L.gid - F.ray_begin, y8, &Q0);
-            write_hit(A, L, BH_HIT_HORIZON, y8);
+            write_hit<P, JET>(A, L, BH_HIT_HORIZON, y8);
             return true;
         }
         return false;
@@ -476,11 +481,15 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         yh[4] = pt;
         yh[7] = pph;
     };
+    // Fraction of the step the jet integral covers: up to an occluding
+    // event, all of it otherwise; < 0: none (render.cpp:107-122, 165-244).
+    double s_jet = 1.0;
     if (F.ns_enabled && rn <= F.ns_R) {
         // neutron-star surface (render.cpp:158-169)
         const DenseC cr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
         what = BH_HIT_STAR;
-        dense_state(dense_crossing(cr, F.ns_R));
+        s_jet = dense_crossing(cr, F.ns_R);
+        dense_state(s_jet);
     } else if (rn <= F.r_stop) {
         what = BH_HIT_HORIZON;             // render.cpp:172-177
     } else if (F.disc_enabled && (double)L.c0 * (double)ax7.cs < 0.0) {
@@ -494,6 +503,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         const double rc = dense_eval(crr, s_end);
         if (rc >= F.r_in && rc <= F.r_out) {
             what = BH_HIT_DISC;
+            s_jet = s_end;
             dense_state(s_end);
         }
     }
@@ -527,6 +537,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             };
             if (f(0.0) <= 0.0) {
                 what = BH_HIT_SUN;
+                s_jet = -1.0;
                 state8(L, ptph, yh);       // already inside at the start of the step
             } else {
                 double prev_s = 0.0;
@@ -539,12 +550,27 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
                             if (f(mid) <= 0.0) hi = mid; else lo = mid;
                         }
                         what = BH_HIT_SUN;
-                        dense_state(0.5 * (lo + hi));
+                        s_jet = 0.5 * (lo + hi);
+                        dense_state(s_jet);
                         break;
                     }
                     prev_s = s;
                 }
             }
+        }
+    }
+    if (JET && s_jet > 0.0) {
+        // Optically thin jet emission along the step (render.cpp:150-152,
+        // 107-122): skipped unless the chord passes within r_bound of the hole.
+        double q0[3], q1[3];
+        bl_cartesian(F.a, (double)L.y[1], (double)L.y[2], (double)L.y[3], q0);
+        bl_cartesian(F.a, rn, (double)yn[2], (double)yn[3], q1);
+        if (segment_distance_to_origin(q0, q1) < F.jet_r_bound) {
+            const DenseC cr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
+            const DenseC ct = dense_coef(hd, L.y[2], yn[2], L.k1[2], k3[2], k4[2], k5[2], k6[2], k7[2]);
+            const DenseC cpr = dense_coef(hd, L.y[4], yn[4], L.k1[4], k3[4], k4[4], k5[4], k6[4], k7[4]);
+            const DenseC cpt = dense_coef(hd, L.y[5], yn[5], L.k1[5], k3[5], k4[5], k5[5], k6[5], k7[5]);
+            L.jet += jet_step_integral(F, cr, ct, cpr, cpt, (double)L.E, (double)L.Lz, hd, s_jet);
         }
     }
     if (what < 0 && rn > F.r_escape) what = BH_HIT_SKY;   // render.cpp:247-251
@@ -592,7 +618,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         state8(L, ptph, yh);
     }
     if (what >= 0) {
-        write_hit(A, L, what, yh);
+        write_hit<P, JET>(A, L, what, yh);
         return true;
     }
     if (P::kMixed && A.deferred &&
@@ -618,12 +644,13 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         dd->steps = L.steps;
         dd->attempts = L.attempts;
         dd->pad = 0;
+        if (JET) A.jet[L.gid] = L.jet;   // the binary64 pass continues the sum
         return true;
     }
     return false;
 }
 
-template <class P, int MAXREG>
+template <class P, int MAXREG, bool JET>
 __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -641,7 +668,7 @@ __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
             const long long id = q_next;
             q_next += q_stride;
             --q_left;
-            active = start_ray<P>(A, L, id);
+            active = start_ray<P, JET>(A, L, id);
         }
         const unsigned want = __ballot_sync(kFull, !active && !done);
         if (want) {
@@ -669,7 +696,7 @@ __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
                             const long long id = q_next;
                             q_next += q_stride;
                             --q_left;
-                            active = start_ray<P>(A, L, id);
+                            active = start_ray<P, JET>(A, L, id);
                         }
                         if (!active && q_left == 0) done = true;
                     }
@@ -681,7 +708,7 @@ __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
             continue;
         }
         if (active) {
-            if (attempt<P>(A, L)) {
+            if (attempt<P, JET>(A, L)) {
                 active = false;
                 if (A.budget) atomicAdd(&A.queue->attempts, (unsigned long long)(L.attempts - L.att0));
             }
@@ -702,7 +729,7 @@ constexpr int kRegMixedWide = 168;
 constexpr int kRegFp64 = 168;
 constexpr int kRegFp64Wide = 232;
 
-template <class P, int MAXREG>
+template <class P, int MAXREG, bool JET>
 cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s) {
     TraceArgs A;
     A.frames = L.frames;
@@ -716,19 +743,38 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.rays_per_thread = L.rays_per_thread < 1 ? 1 : L.rays_per_thread;
     A.refill = L.refill < 1 ? 1 : (L.refill > 32 ? 32 : L.refill);
     A.budget = L.budget;
-    trace_kernel<P, MAXREG><<<grid, block, 0, s>>>(A);
+    A.jet = L.jet;
+    trace_kernel<P, MAXREG, JET><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
 }
 
 const void* kernel_of(int precision, int variant, int resume) {
     if (precision == BH_PRECISION_MIXED && !resume)
-        return variant ? (const void*)trace_kernel<Mixed, kRegMixedWide> : (const void*)trace_kernel<Mixed, kRegMixed>;
-    return variant ? (const void*)trace_kernel<Fp64, kRegFp64Wide> : (const void*)trace_kernel<Fp64, kRegFp64>;
+        return variant ? (const void*)trace_kernel<Mixed, kRegMixedWide, false>
+                       : (const void*)trace_kernel<Mixed, kRegMixed, false>;
+    return variant ? (const void*)trace_kernel<Fp64, kRegFp64Wide, false>
+                   : (const void*)trace_kernel<Fp64, kRegFp64, false>;
 }
 
+// The kernels of launches with a jet accumulate its emission per ray; the
+// others are compiled without that code.
+template <bool JET>
 cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, int block, int variant, cudaStream_t s) {
-    return variant ? launch_t<Fp64, kRegFp64Wide>(L, resume, grid, block, s)
-                   : launch_t<Fp64, kRegFp64>(L, resume, grid, block, s);
+    return variant ? launch_t<Fp64, kRegFp64Wide, JET>(L, resume, grid, block, s)
+                   : launch_t<Fp64, kRegFp64, JET>(L, resume, grid, block, s);
+}
+
+template <bool JET>
+cudaError_t launch_trace_t(const TraceLaunch& L, cudaStream_t stream) {
+    if (L.precision == BH_PRECISION_MIXED) {
+        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide, JET>(L, 0, L.grid, L.block_size, stream)
+                                      : launch_t<Mixed, kRegMixed, JET>(L, 0, L.grid, L.block_size, stream);
+        if (e != cudaSuccess) return e;
+        if (L.resume_event) cudaEventRecord(L.resume_event, stream);
+        // The deferred rays, in binary64: every block reads the deferred count.
+        return launch_fp64<JET>(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);
+    }
+    return launch_fp64<JET>(L, 0, L.grid, L.block_size, L.reg_variant, stream);
 }
 
 }  // namespace
@@ -736,15 +782,7 @@ cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, int block, i
 size_t deferred_record_bytes() { return sizeof(Deferred); }
 
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
-    if (L.precision == BH_PRECISION_MIXED) {
-        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide>(L, 0, L.grid, L.block_size, stream)
-                                      : launch_t<Mixed, kRegMixed>(L, 0, L.grid, L.block_size, stream);
-        if (e != cudaSuccess) return e;
-        if (L.resume_event) cudaEventRecord(L.resume_event, stream);
-        // The deferred rays, in binary64: every block reads the deferred count.
-        return launch_fp64(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);
-    }
-    return launch_fp64(L, 0, L.grid, L.block_size, L.reg_variant, stream);
+    return L.jet ? launch_trace_t<true>(L, stream) : launch_trace_t<false>(L, stream);
 }
 
 int trace_blocks_per_sm(int precision, int block_size, int variant) {

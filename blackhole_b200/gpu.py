@@ -67,6 +67,8 @@ def load_library():
             "bh_gpu_fma_peak": (C.c_int, [C.c_int, C.c_int, P(C.c_double)]),
             "bh_gpu_trace_noalloc": (C.c_int, [C.c_int, cfg_p, C.c_void_p, C.c_void_p]),
             "bh_display_default": (None, [P(abi.bh_display)]),
+            "bh_jet_configure": (None, [P(abi.bh_jet), C.c_double, C.c_double, C.c_double]),
+            "bh_render_config_setup_jet": (C.c_int, [cfg_p]),
             "bh_gpu_develop": (C.c_int, [ctx_p, P(abi.bh_xyz), C.c_int, C.c_int, P(abi.bh_display),
                                          P(C.c_uint8), P(C.c_double)]),
             "bh_gpu_render_rgb": (C.c_int, [ctx_p, cfg_p, P(abi.bh_display), P(C.c_uint8), P(C.c_double), st_p]),

@@ -155,3 +155,44 @@ def photon_ring_4096(precision: int = abi.PRECISION_MIXED, size: int = 4096) -> 
     )
     cfg.cam.yaw = math.atan(critical_curve_prograde_edge(0.998, math.radians(75.0)) / R_OBS)
     return cfg
+
+
+def _jet_preset(cfg: RenderConfig, z_top: float, gamma_max: float) -> RenderConfig:
+    """Jets on, configured the way the CLI does (main.cpp:399-423), and the
+    escape sphere outside them (main.cpp:881-890)."""
+    cfg.jet_enabled = True
+    cfg.jet.z_top = z_top
+    cfg.jet.gamma_max = gamma_max
+    cfg.setup_jet()
+    far = cfg.cam.r * 3.0 + 100.0
+    if cfg.jet_enabled:
+        far = max(far, cfg.jet.r_bound * 1.5)
+    cfg.r_escape = far
+    return cfg
+
+
+def quasar_jets(width: int = 320, height: int = 180, precision: int = abi.PRECISION_FP64) -> RenderConfig:
+    """The reference's `quasar` preset (main.cpp:300-330): a = 0.998,
+    M = 1e9 M_sun, 84 deg, r_cam 80 M, fov 0.90, disc to 20 M at 0.5
+    Eddington, Blandford-Znajek jets to z = 130 M with Gamma_max = 10; the
+    reference's galactic sky and stop radius, 1 sample per pixel."""
+    cfg = RenderConfig(
+        M_kg=1.0e9 * M_SUN, spin=0.998,
+        cam=Camera(r=80.0, theta=math.radians(84.0), phi=0.0, fov=0.90),
+        width=width, height=height, sqrt_spp=1, disc_r_out=20.0, eddington=0.5,
+        quiet=True, precision=precision,
+    )
+    return _jet_preset(cfg, 130.0, 10.0)
+
+
+def m87_jets(width: int = 320, height: int = 180, precision: int = abi.PRECISION_FP64) -> RenderConfig:
+    """The reference's `m87` preset (main.cpp:252-267): a = 0.94,
+    M = 6.5e9 M_sun, 17 deg, r_cam 120 M, fov 0.78, disc to 30 M at 1e-5
+    Eddington, jets to z = 130 M with Gamma_max = 8."""
+    cfg = RenderConfig(
+        M_kg=6.5e9 * M_SUN, spin=0.94,
+        cam=Camera(r=120.0, theta=math.radians(17.0), phi=0.0, fov=0.78),
+        width=width, height=height, sqrt_spp=1, disc_r_out=30.0, eddington=1e-5,
+        quiet=True, precision=precision,
+    )
+    return _jet_preset(cfg, 130.0, 8.0)

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define BH_GPU_ABI_VERSION 1
+#define BH_GPU_ABI_VERSION 2
 
 /* Status codes. */
 enum {
@@ -114,6 +114,22 @@ typedef struct bh_neutron_star {  /* bh::NeutronStar (neutronstar.h:43-70) */
     int32_t reserved;
 } bh_neutron_star;
 
+/* bh::Jet (jet.h:96-315) without its `enabled` flag, which is
+   bh_render_config.jet_enabled.  The first block is the prescribed model; the
+   second is what Jet::configure (jet.h:262-312) sets from the spin and the
+   accretion rate: fill it with bh_jet_configure or bh_render_config_setup_jet
+   before rendering (a zero j_nu0 renders no jet). */
+typedef struct bh_jet {
+    double z_base, z_top, R_base, k;       /* geometry: R(z) = R_base (z / z_base)^k, GM/c^2  */
+    double gamma_max, z_sat;               /* bulk Lorentz factor law                          */
+    double alpha;                          /* synchrotron index, S_nu ~ nu^-alpha              */
+    double u_peak, u_wid, spine, spine_wid;/* limb-brightened radial profile                   */
+    double zeta;                           /* re-acceleration index                            */
+    double eps_rad, phi_flux;              /* radiated fraction, horizon flux (MAD = 50)       */
+    /* ---- set by configure ---- */
+    double a, Omega_F, P_jet, L_rad, j_nu0, r_bound, volume_rg3;
+} bh_jet;
+
 /* bh::RenderConfig (render.h:15-53) plus the GPU extensions at the end. */
 typedef struct bh_render_config {
     uint32_t struct_size;    /* sizeof(bh_render_config) as the caller compiled it */
@@ -136,7 +152,7 @@ typedef struct bh_render_config {
     bh_sun sun;
     bh_hotspot hotspot;
     bh_neutron_star star;
-    int32_t jet_enabled;     /* jets are not built: must be 0 */
+    int32_t jet_enabled;     /* bh::Jet::enabled; the model is `jet` below */
     int32_t reserved0;
 
     double observer_time;
@@ -156,6 +172,7 @@ typedef struct bh_render_config {
     double stop_epsilon;     /* BH_STOP_RELATIVE only                            */
     double mixed_rtol;       /* tolerances of the MIXED path; 0 = max(rtol, 1e-6) */
     double mixed_atol;       /*                               0 = max(atol, 1e-8) */
+    bh_jet jet;              /* bh::RenderConfig::jet (render.h:37)              */
 } bh_render_config;
 
 /* bh::RenderStats (render.h:55-69) plus extensions. */
@@ -193,6 +210,7 @@ typedef struct bh_ray_result {
     int32_t reserved;
     double max_norm;         /* worst relative null norm along the ray          */
     double max_q;            /* worst relative Carter drift along the ray       */
+    double jet;              /* jet emission picked up, Hit::jet (render.cpp:41) */
 } bh_ray_result;
 
 /* Launch shape of the persistent trace kernel (the autotuner's search space). */
@@ -209,9 +227,20 @@ typedef struct bh_ctx bh_ctx;
 
 int  bh_gpu_abi_version(void);
 
-/* The reference's defaults (render.h:15-53, scene.h:343-351) plus
+/* The reference's defaults (render.h:15-53, scene.h:343-351, jet.h:96-146) plus
    BH_PRECISION_FP64, BH_SKY_GALACTIC, BH_STOP_REFERENCE, milky_way = 1. */
 void bh_render_config_default(bh_render_config* cfg);
+
+/* Jet::configure (jet.h:262-312): Blandford-Znajek power of spin `spin` for
+   an accretion flow of mdot_c2 watts around a hole of gravitational radius
+   r_g_m metres, and the emissivity normalisation that radiates eps_rad of it. */
+void bh_jet_configure(bh_jet* jet, double spin, double mdot_c2, double r_g_m);
+
+/* The CLI's jet set-up (main.cpp:399-423) on a config: with jet_enabled, jets
+   are switched off for a neutron star or without a disc (no accretion flow),
+   z_sat is capped at 0.7 z_top, the jet is configured from the disc's
+   accretion rate, and switched off when the hole has no rotational power. */
+int  bh_render_config_setup_jet(bh_render_config* cfg);
 
 int  bh_gpu_create(int device, bh_ctx** out);
 void bh_gpu_destroy(bh_ctx* ctx);
@@ -301,6 +330,8 @@ typedef struct bh_trace_record {
    before any stream capture); every call clears the counters it needs at
    zero, and all calls share the one array, so calls whose work overlaps on
    the GPU (other streams, other host threads) race - serialise them.
+   A config with a jet returns BH_ERR_UNSUPPORTED (the jet's emission is a
+   per-ray sum this entry point has no scratch for).
    Stars, disc temperature and pixels are not computed (no shading): the
    records equal the trace part of bh_gpu_trace_rays for the same config and
    default launch shape.  Records are in work order: ray id = p * S^2 + k for

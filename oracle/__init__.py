@@ -78,6 +78,11 @@ def _declare(lib, prefix: str) -> None:
     fn("render", C.c_int, _CFG, C.POINTER(abi.bh_xyz), _ST)
     fn("render_rows", C.c_int, _CFG, C.POINTER(C.c_int), C.c_int, C.c_int,
        C.POINTER(abi.bh_xyz), _ST, _PD)
+    _PJ = C.POINTER(abi.bh_jet)
+    fn("jet_configure", None, _PJ, _D, _D, _D)
+    fn("powerlaw_xyz", None, _D, _PD)
+    fn("jet_shape", _D, _PJ, _D, _D)
+    fn("jet_four_velocity", None, _PJ, _D, _D, _D, _PD)
     _PX = C.POINTER(abi.bh_xyz)
     _U8 = C.POINTER(C.c_uint8)
     if prefix == "orc_":
@@ -255,6 +260,26 @@ class Port:
         if rc != 0:
             raise RuntimeError(f"{self.prefix}render_rows failed: {abi.STATUS_NAMES.get(rc, rc)}")
         return out, st, setup.value
+
+    # -- jets (jet.h:77-315) --------------------------------------------------------
+    def jet_configure(self, jet_c, spin, mdot_c2, r_g_m):
+        """Jet::configure on a copy of a bh_jet; returns the copy."""
+        j = abi.bh_jet.from_buffer_copy(jet_c)
+        self._f("jet_configure")(C.byref(j), spin, mdot_c2, r_g_m)
+        return j
+
+    def powerlaw_xyz(self, alpha):
+        out = np.zeros(3)
+        self._f("powerlaw_xyz")(alpha, _ptr(out))
+        return out
+
+    def jet_shape(self, jet_c, z, rho):
+        return self._f("jet_shape")(C.byref(jet_c), z, rho)
+
+    def jet_four_velocity(self, jet_c, a, r, th):
+        out = np.zeros(4)
+        self._f("jet_four_velocity")(C.byref(jet_c), a, r, th, _ptr(out))
+        return out
 
     # -- display transform (image.cpp:22-191) ------------------------------------
     @staticmethod

@@ -770,6 +770,172 @@ static void ray_direction(const bh_camera* cam, double sx, double sy, double asp
 }
 
 /* ======================================================================== */
+/* Jets (jet.h:77-315) and their colour (spectrum.cpp:77-92)                */
+/* ======================================================================== */
+
+static double horizon_angular_velocity(double a) {   /* kerr.h:204-207 */
+    const double rp = horizon_outer(a);
+    return (rp > 0.0) ? a / (2.0 * rp) : 0.0;
+}
+
+/* jet.h:81-87 */
+static double blandford_znajek_power(double a, double mdot_c2, double phi, double kappa) {
+    const double OmH = horizon_angular_velocity(a);
+    const double x = OmH * OmH;
+    const double f = 1.0 + 1.38 * x - 9.2 * x * x;
+    return (kappa / (4.0 * ORC_PI)) * phi * phi * x * dmax(0.0, f) * mdot_c2;
+}
+
+static double smoothstep01(double t) {   /* jet.h:91-94 */
+    t = dclamp(t, 0.0, 1.0);
+    return t * t * (3.0 - 2.0 * t);
+}
+
+static double jet_radius(const bh_jet* j, double z_abs) {
+    return j->R_base * pow(dmax(z_abs, 1e-6) / j->z_base, j->k);
+}
+static double jet_gamma_at(const bh_jet* j, double z_abs) {
+    const double t = dmin(1.0, pow(dmax(z_abs, 1e-6) / j->z_sat, j->k));
+    return 1.0 + (j->gamma_max - 1.0) * t;
+}
+static double jet_speed_at(const bh_jet* j, double z_abs) {
+    const double G = jet_gamma_at(j, z_abs);
+    return sqrt(dmax(0.0, 1.0 - 1.0 / (G * G)));
+}
+static double jet_radial_profile(const bh_jet* j, double u) {
+    const double s = (u - j->u_peak) / j->u_wid;
+    const double t = u / j->spine_wid;
+    return exp(-s * s) + j->spine * exp(-t * t);
+}
+
+/* jet.h:194-207 */
+static double jet_shape(const bh_jet* j, double z, double rho) {
+    const double az = fabs(z);
+    if (az <= j->z_base || az >= j->z_top) return 0.0;
+    const double R = jet_radius(j, az);
+    const double f = jet_radial_profile(j, rho / R);
+    if (f < 1e-9) return 0.0;
+    const double g = pow(jet_gamma_at(j, az) / jet_gamma_at(j, j->z_base), -(2.0 + j->alpha)) *
+                     pow(R / j->R_base, -(3.0 + j->alpha)) * pow(az / j->z_base, j->zeta);
+    const double ramp = smoothstep01((az - j->z_base) / (0.5 * j->z_base)) *
+                        smoothstep01((j->z_top - az) / (0.15 * j->z_top));
+    return f * g * ramp;
+}
+
+/* jet.h:215-240: the plasma four-velocity, built in the ZAMO frame. */
+static void jet_four_velocity(const bh_jet* j, const geom_t* g, double u[4]) {
+    const tetrad_t T = zamo_tetrad(g);
+    const double lapse = sqrt(g->Sigma * g->Delta / g->A);
+    const double omega = 2.0 * g->a * g->r / g->A;
+    const double sqrt_gpp = g->sn * sqrt(g->A / g->Sigma);
+    const double z = g->r * g->cs;
+    const double v = jet_speed_at(j, fabs(z));
+    double v_phi = (j->Omega_F - omega) * sqrt_gpp / dmax(lapse, 1e-12);
+    v_phi = dclamp(v_phi, -0.5 * v, 0.5 * v);
+    const double v_pol = sqrt(dmax(0.0, v * v - v_phi * v_phi));
+    const double sgn = (g->cs >= 0.0) ? 1.0 : -1.0;
+    const double d_r = sgn * g->cs;
+    const double d_th = -sgn * g->sn;
+    const double G = 1.0 / sqrt(dmax(1e-12, 1.0 - v * v));
+    for (int mu = 0; mu < 4; ++mu)
+        u[mu] = G * (T.e[0][mu] + v_pol * (d_r * T.e[1][mu] + d_th * T.e[2][mu]) + v_phi * T.e[3][mu]);
+}
+
+/* jet.h:262-312 */
+static void jet_configure(bh_jet* j, double spin, double mdot_c2, double r_g_m) {
+    const double nu_0 = PH_C / 550e-9, nu_lo = 1.0e9, nu_hi = 1.0e17;
+    j->a = spin;
+    j->Omega_F = 0.5 * horizon_angular_velocity(spin);
+    j->P_jet = blandford_znajek_power(spin, mdot_c2, j->phi_flux, 0.053);
+    j->L_rad = j->eps_rad * j->P_jet;
+    j->r_bound = sqrt(j->z_top * j->z_top + jet_radius(j, j->z_top) * jet_radius(j, j->z_top)) * 1.05;
+    double C_f = 0.0;
+    {
+        const int N = 2000;
+        const double du = 3.0 / N;
+        for (int i = 0; i < N; ++i) {
+            const double u = (i + 0.5) * du;
+            C_f += jet_radial_profile(j, u) * u * du;
+        }
+    }
+    double V = 0.0;
+    {
+        const int N = 4000;
+        const double dz = (j->z_top - j->z_base) / N;
+        for (int i = 0; i < N; ++i) {
+            const double z = j->z_base + (i + 0.5) * dz;
+            const double R = jet_radius(j, z);
+            const double gz = pow(jet_gamma_at(j, z) / jet_gamma_at(j, j->z_base), -(2.0 + j->alpha)) *
+                              pow(R / j->R_base, -(3.0 + j->alpha)) * pow(z / j->z_base, j->zeta);
+            const double ramp = smoothstep01((z - j->z_base) / (0.5 * j->z_base)) *
+                                smoothstep01((j->z_top - z) / (0.15 * j->z_top));
+            V += gz * ramp * R * R * dz;
+        }
+        V *= 2.0 * (2.0 * ORC_PI) * C_f;
+    }
+    j->volume_rg3 = V;
+    const double V_m3 = V * r_g_m * r_g_m * r_g_m;
+    if (!(V_m3 > 0.0) || !(j->L_rad > 0.0)) { j->j_nu0 = 0.0; return; }
+    const double A = j->L_rad / (4.0 * ORC_PI * V_m3);
+    const double p = 1.0 - j->alpha;
+    const double band = (fabs(p) > 1e-9) ? (pow(nu_hi, p) - pow(nu_lo, p)) / p : log(nu_hi / nu_lo);
+    j->j_nu0 = A / (pow(nu_0, j->alpha) * band) * r_g_m;
+}
+
+/* spectrum.cpp:77-92: the colour of a unit power law I_nu ~ nu^-alpha. */
+static void powerlaw_xyz(double alpha, double out[3]) {
+    const double lambda_0 = 550e-9;
+    out[0] = out[1] = out[2] = 0.0;
+    const double lo = 360.0, hi = 830.0, dl = 1.0;
+    for (double nm = lo; nm <= hi; nm += dl) {
+        const double lam = nm * 1e-9;
+        const double I_l = PH_C * pow(lam / lambda_0, alpha) / (lam * lam);
+        const double w = I_l * dl * 1e-9;
+        out[0] += w * cie_x(nm);
+        out[1] += w * cie_y(nm);
+        out[2] += w * cie_z(nm);
+    }
+}
+
+/* render.cpp:55-62 */
+static double segment_distance_to_origin(const double p0[3], const double p1[3]) {
+    const double d[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    const double dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    double t = 0.0;
+    if (dd > 0.0) t = dclamp(-(p0[0] * d[0] + p0[1] * d[1] + p0[2] * d[2]) / dd, 0.0, 1.0);
+    const double q[3] = {p0[0] + t * d[0], p0[1] + t * d[1], p0[2] + t * d[2]};
+    return sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+}
+
+/* render.cpp:44-50: four-point Gauss-Legendre on [0, 1]. */
+static const double kGLx[4] = {0.06943184420297371, 0.33000947820757187, 0.66999052179242813,
+                               0.93056815579702629};
+static const double kGLw[4] = {0.17392742256872693, 0.32607257743127307, 0.32607257743127307,
+                               0.17392742256872693};
+
+/* render.cpp:107-122: the transfer integral over the part [0, s_end] of one step. */
+static void sample_jet(const bh_jet* j, double a, const dense_t* dense, double h_step, double s_end,
+                       double* acc) {
+    if (s_end <= 0.0) return;
+    double sum = 0.0;
+    for (int q = 0; q < 4; ++q) {
+        double ys[8];
+        dense_eval(dense, kGLx[q] * s_end, ys);
+        const double z = ys[YR] * cos(ys[YTH]);
+        const double rho = sqrt(ys[YR] * ys[YR] + a * a) * sin(ys[YTH]);
+        const double sh = jet_shape(j, z, rho);
+        if (sh <= 0.0) continue;
+        const geom_t gg = geom_at(a, ys[YR], ys[YTH]);
+        double u[4];
+        jet_four_velocity(j, &gg, u);
+        const double gf = redshift_factor(ys, u);
+        if (gf <= 0.0) continue;
+        sum += kGLw[q] * sh * pow(gf, 2.0 + j->alpha);
+    }
+    *acc += j->j_nu0 * sum * h_step * s_end;
+}
+
+/* ======================================================================== */
 /* Tracer and shading                                                       */
 /* ======================================================================== */
 
@@ -781,6 +947,8 @@ typedef struct {
     int have_stars;
     tetrad_t tet;
     double psf_sigma, aspect;
+    int have_jet;
+    double jet_colour[3];
 } scene_t;
 
 typedef struct { int what; double y[8]; double jet; int steps, attempts; double q_drift, norm_rel; } hit_t;
@@ -813,7 +981,7 @@ static double ns_temperature_at(const bh_neutron_star* st, double theta, double 
     return st->T_eff;
 }
 
-/* render.cpp:69-260 (the jet is not modelled: config must have it off). */
+/* render.cpp:69-260 */
 static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* local) {
     const bh_render_config* cfg = sc->cfg;
     const double a = cfg->spin;
@@ -858,6 +1026,8 @@ static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* loca
             hit.q_drift = dmax(hit.q_drift, fabs(iv.Q - iv0.Q) / Q0);
         }
         bl_to_cartesian(a, ynew[YR], ynew[YTH], ynew[YPH], p1);
+        /* render.cpp:150-152: most steps are nowhere near the jet */
+        const int near_jet = sc->have_jet && segment_distance_to_origin(p0, p1) < cfg->jet.r_bound;
 
         /* render.cpp:158-169: neutron-star surface */
         if (cfg->star.enabled && ynew[YR] <= cfg->star.R) {
@@ -868,12 +1038,14 @@ static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* loca
                 if (ys[YR] <= cfg->star.R) hi = mid; else lo = mid;
             }
             const double s_end = 0.5 * (lo + hi);
+            if (near_jet) sample_jet(&cfg->jet, a, &dense, dense.h, s_end, &hit.jet);
             hit.what = BH_HIT_STAR;
             dense_eval(&dense, s_end, hit.y);
             return hit;
         }
         /* render.cpp:172-177: horizon */
         if (ynew[YR] <= r_stop) {
+            if (near_jet) sample_jet(&cfg->jet, a, &dense, dense.h, 1.0, &hit.jet);
             hit.what = BH_HIT_HORIZON;
             memcpy(hit.y, ynew, sizeof ynew);
             return hit;
@@ -894,6 +1066,7 @@ static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* loca
                 double yc[8];
                 dense_eval(&dense, s_end, yc);
                 if (disc_contains(&sc->disc, yc[YR])) {
+                    if (near_jet) sample_jet(&cfg->jet, a, &dense, dense.h, s_end, &hit.jet);
                     hit.what = BH_HIT_DISC;
                     memcpy(hit.y, yc, sizeof yc);
                     return hit;
@@ -933,6 +1106,7 @@ static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* loca
                             if (fm <= 0.0) hi2 = mid; else lo = mid;
                         }
                         const double s_end = 0.5 * (lo + hi2);
+                        if (near_jet) sample_jet(&cfg->jet, a, &dense, dense.h, s_end, &hit.jet);
                         hit.what = BH_HIT_SUN;
                         dense_eval(&dense, s_end, hit.y);
                         return hit;
@@ -942,6 +1116,8 @@ static hit_t trace(const scene_t* sc, const double dir[3], bh_render_stats* loca
 #undef SUN_F
             }
         }
+        /* render.cpp:244: nothing stopped the ray inside this step */
+        if (near_jet) sample_jet(&cfg->jet, a, &dense, dense.h, 1.0, &hit.jet);
         /* render.cpp:247-251: escape */
         if (ynew[YR] > cfg->r_escape) {
             hit.what = BH_HIT_SKY;
@@ -1068,8 +1244,11 @@ static void shade_hit(const scene_t* sc, const hit_t* hit, bh_render_stats* loca
 static int scene_init(scene_t* sc, const bh_render_config* cfg) {
     memset(sc, 0, sizeof *sc);
     if (!cfg || cfg->width <= 0 || cfg->height <= 0) return BH_ERR_INVALID_ARG;
-    if (cfg->jet_enabled) return BH_ERR_UNSUPPORTED;
     sc->cfg = cfg;
+    if (cfg->jet_enabled) {
+        sc->have_jet = 1;
+        powerlaw_xyz(cfg->jet.alpha, sc->jet_colour);   /* render.cpp:417 */
+    }
     if (cfg->disc_enabled) {
         disc_init(&sc->disc, cfg->M_kg, cfg->spin, cfg->disc_r_out, cfg->eddington, cfg->disc_sense);
         sc->have_disc = 1;
@@ -1131,6 +1310,12 @@ static int run_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                     const hit_t hit = trace(&sc, dir, &local);
                     double c[3], g, sdir[3];
                     shade_hit(&sc, &hit, &local, c, &g, sdir);
+                    if (hit.jet > 0.0) {   /* render.cpp:384-392 */
+                        ++local.jet_rays;
+                        c[0] += sc.jet_colour[0] * hit.jet;
+                        c[1] += sc.jet_colour[1] * hit.jet;
+                        c[2] += sc.jet_colour[2] * hit.jet;
+                    }
                     acc[0] += c[0]; acc[1] += c[1]; acc[2] += c[2];
                     if (rays) {
                         bh_ray_result* o = &rays[ridx++];
@@ -1144,6 +1329,7 @@ static int run_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                         o->reserved = 0;
                         o->max_norm = hit.norm_rel;
                         o->max_q = hit.q_drift;
+                        o->jet = hit.jet;
                     }
                 }
             }
@@ -1443,4 +1629,16 @@ void orc_develop(const bh_xyz* px, long n, double exposure, int tonemap, double 
         }
         for (int ch = 0; ch < 3; ++ch) out[i * 3 + ch] = (uint8_t)lround(255.0 * srgb_encode(v[ch]));
     }
+}
+
+
+/* ---- jets ---------------------------------------------------------------- */
+void orc_jet_configure(bh_jet* jet, double spin, double mdot_c2, double r_g_m) {
+    jet_configure(jet, spin, mdot_c2, r_g_m);
+}
+void orc_powerlaw_xyz(double alpha, double out3[3]) { powerlaw_xyz(alpha, out3); }
+double orc_jet_shape(const bh_jet* jet, double z, double rho) { return jet_shape(jet, z, rho); }
+void orc_jet_four_velocity(const bh_jet* jet, double a, double r, double th, double out4[4]) {
+    const geom_t g = geom_at(a, r, th);
+    jet_four_velocity(jet, &g, out4);
 }

@@ -78,6 +78,12 @@ int    orc_trace_rays(const bh_render_config* cfg, int x0, int y0, int w, int h,
 int    orc_render_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                          bh_xyz* out, bh_render_stats* stats);
 
+/* Jets (jet.h:77-315, spectrum.cpp:77-92). */
+void   orc_jet_configure(bh_jet* jet, double spin, double mdot_c2, double r_g_m);
+void   orc_powerlaw_xyz(double alpha, double out3[3]);
+double orc_jet_shape(const bh_jet* jet, double z, double rho);
+void   orc_jet_four_velocity(const bh_jet* jet, double a, double r, double th, double out4[4]);
+
 /* Display transform (image.cpp:22-191).  tonemap: 0 Linear, 1 Reinhard,
    2 ACES, 3 Log, 4 HDR (img::ToneMap order). */
 double orc_auto_exposure(const bh_xyz* px, long n, double key);

@@ -83,7 +83,28 @@ bh::RenderConfig to_ref(const bh_render_config& c) {
     r.star.cap_T = c.star.cap_T;
     r.star.cap_phase0 = c.star.cap_phase0;
     r.star.two_caps = c.star.two_caps != 0;
-    r.jet.enabled = false;
+    r.jet.enabled = c.jet_enabled != 0;
+    r.jet.z_base = c.jet.z_base;
+    r.jet.z_top = c.jet.z_top;
+    r.jet.R_base = c.jet.R_base;
+    r.jet.k = c.jet.k;
+    r.jet.gamma_max = c.jet.gamma_max;
+    r.jet.z_sat = c.jet.z_sat;
+    r.jet.alpha = c.jet.alpha;
+    r.jet.u_peak = c.jet.u_peak;
+    r.jet.u_wid = c.jet.u_wid;
+    r.jet.spine = c.jet.spine;
+    r.jet.spine_wid = c.jet.spine_wid;
+    r.jet.zeta = c.jet.zeta;
+    r.jet.eps_rad = c.jet.eps_rad;
+    r.jet.phi_flux = c.jet.phi_flux;
+    r.jet.a = c.jet.a;
+    r.jet.Omega_F = c.jet.Omega_F;
+    r.jet.P_jet = c.jet.P_jet;
+    r.jet.L_rad = c.jet.L_rad;
+    r.jet.j_nu0 = c.jet.j_nu0;
+    r.jet.r_bound = c.jet.r_bound;
+    r.jet.volume_rg3 = c.jet.volume_rg3;
     r.observer_time = c.observer_time;
     r.rtol = c.rtol;
     r.atol = c.atol;
@@ -96,8 +117,8 @@ bh::RenderConfig to_ref(const bh_render_config& c) {
 
 int check_cfg(const bh_render_config* c) {
     if (!c || c->width <= 0 || c->height <= 0) return BH_ERR_INVALID_ARG;
-    // The reference has one sky, one stop rule and no jet hook here.
-    if (c->jet_enabled || c->sky_mode != BH_SKY_GALACTIC || c->stop_mode != BH_STOP_REFERENCE)
+    // The reference has one sky and one stop rule.
+    if (c->sky_mode != BH_SKY_GALACTIC || c->stop_mode != BH_STOP_REFERENCE)
         return BH_ERR_UNSUPPORTED;
     return BH_OK;
 }
@@ -137,7 +158,7 @@ struct Scene {
         tet = bh::zamo_tetrad(gcam);
         aspect = static_cast<double>(cfg.width) / cfg.height;
         psf_sigma = 0.55 * (cfg.cam.fov / cfg.width);
-        jet_colour = spec::XYZ{};
+        jet_colour = cfg.jet.enabled ? spec::powerlaw_xyz(cfg.jet.alpha) : spec::XYZ{};   // render.cpp:417
     }
 };
 
@@ -271,6 +292,7 @@ int ref_trace_rays(const bh_render_config* c, int x0, int y0, int w, int h, bh_r
                     o.steps = static_cast<int32_t>(rs.steps);
                     o.max_norm = rs.max_norm_error;
                     o.max_q = rs.max_carter_drift;
+                    o.jet = hit.jet;
                     for (int i = 0; i < 8; ++i) o.y[i] = hit.y[i];
                     o.xyz.x = col.x; o.xyz.y = col.y; o.xyz.z = col.z;
                     // The fields shade_hit computes on the way (render.cpp:275-325).
@@ -380,6 +402,36 @@ int ref_sky_radiance(int count, uint64_t seed, int milky_way, const double* dirs
         out3[3 * i] = c.x; out3[3 * i + 1] = c.y; out3[3 * i + 2] = c.z;
     }
     return BH_OK;
+}
+
+// Jets: Jet::configure, the power-law colour, the shape and the four-velocity.
+namespace {
+bh::Jet jet_of(const bh_jet& j) {
+    bh::Jet o;
+    o.z_base = j.z_base; o.z_top = j.z_top; o.R_base = j.R_base; o.k = j.k;
+    o.gamma_max = j.gamma_max; o.z_sat = j.z_sat; o.alpha = j.alpha;
+    o.u_peak = j.u_peak; o.u_wid = j.u_wid; o.spine = j.spine; o.spine_wid = j.spine_wid;
+    o.zeta = j.zeta; o.eps_rad = j.eps_rad; o.phi_flux = j.phi_flux;
+    o.a = j.a; o.Omega_F = j.Omega_F; o.P_jet = j.P_jet; o.L_rad = j.L_rad; o.j_nu0 = j.j_nu0;
+    o.r_bound = j.r_bound; o.volume_rg3 = j.volume_rg3;
+    return o;
+}
+}  // namespace
+
+void ref_jet_configure(bh_jet* jet, double spin, double mdot_c2, double r_g_m) {
+    bh::Jet j = jet_of(*jet);
+    j.configure(spin, mdot_c2, r_g_m);
+    jet->a = j.a; jet->Omega_F = j.Omega_F; jet->P_jet = j.P_jet; jet->L_rad = j.L_rad;
+    jet->j_nu0 = j.j_nu0; jet->r_bound = j.r_bound; jet->volume_rg3 = j.volume_rg3;
+}
+void ref_powerlaw_xyz(double alpha, double out3[3]) {
+    const spec::XYZ c = spec::powerlaw_xyz(alpha);
+    out3[0] = c.x; out3[1] = c.y; out3[2] = c.z;
+}
+double ref_jet_shape(const bh_jet* jet, double z, double rho) { return jet_of(*jet).shape(z, rho); }
+void ref_jet_four_velocity(const bh_jet* jet, double a, double r, double th, double out4[4]) {
+    const auto u = jet_of(*jet).four_velocity(bh::geom_at(a, r, th));
+    for (int i = 0; i < 4; ++i) out4[i] = u[i];
 }
 
 // The display transform (image.cpp:22-191), through the reference's own img::.

@@ -1,12 +1,14 @@
 """Parity cases shared by the golden generator and the tests.
 
 Every case is a RenderConfig plus a pixel window.  Only the reference's own
-rules (BH_SKY_GALACTIC, BH_STOP_REFERENCE, no jet) appear here, because the
-golden vectors come from the reference renderer itself.
+rules (BH_SKY_GALACTIC, BH_STOP_REFERENCE) appear here, because the golden
+vectors come from the reference renderer itself.  The jet cases are the
+reference CLI's `quasar` and `m87` presets with their jets configured as the
+CLI does it.
 """
 import math
 
-from blackhole_b200 import abi
+from blackhole_b200 import abi, workloads
 from blackhole_b200.config import M_SUN, Camera, HotSpot, NeutronStar, RenderConfig, SunBody
 
 
@@ -74,6 +76,8 @@ CASES = {
     "a0998_i85_ring": (lambda: edge_on_a0998(), (468, 500, 40, 24)),
     "sun_hotspot_spp2": (sun_hotspot_spp2, (0, 0, 24, 16)),
     "neutron_star": (neutron_star, (0, 0, 24, 24)),
+    "quasar_jets": (lambda: workloads.quasar_jets(320, 180), (150, 40, 20, 12)),
+    "m87_jets": (lambda: workloads.m87_jets(320, 180), (150, 60, 20, 12)),
 }
 
 # A whole small frame through the reference's own bh::render (pixels).

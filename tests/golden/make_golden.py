@@ -3,7 +3,7 @@
 Runs the reference renderer compiled from its own sources (oracle/_ref, built
 by oracle/Makefile from the reference tree) on the cases of cases.py and
 stores per-sample trace/shade results (class, steps, final state, g, sky
-direction, XYZ) and one whole frame of pixels.  Usage, where the reference
+direction, XYZ, jet emission) and one whole frame of pixels.  Usage, where the reference
 tree exists:
 
     python tests/golden/make_golden.py
@@ -32,7 +32,7 @@ def main():
         np.savez_compressed(
             os.path.join(HERE, f"{name}.npz"),
             window=np.array([x0, y0, w, h]), what=arr["what"].astype(np.int8),
-            steps=arr["steps"], y=arr["y"], g=arr["g"], dir=arr["dir"], xyz=arr["xyz"],
+            steps=arr["steps"], y=arr["y"], g=arr["g"], dir=arr["dir"], xyz=arr["xyz"], jet=arr["jet"],
             stats=np.array([st.rays, st.steps, st.captured, st.disc_hits, st.sun_hits, st.star_hits,
                             st.escaped, st.exhausted]),
             drift=np.array([st.max_norm_error, st.max_carter_drift]),

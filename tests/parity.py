@@ -49,6 +49,15 @@ def compare(gpu: np.ndarray, chk: dict) -> dict:
         out["Y_rel"] = np.abs(gpu["xyz"][lit, 1] - yc) / np.abs(yc)
     else:
         out["Y_rel"] = np.zeros(0)
+    if "jet" in chk and "jet" in gpu.dtype.names:
+        jc_all = np.asarray(chk["jet"])
+        jl = same & (jc_all > 0)
+        out["jet_rel"] = (np.abs(gpu["jet"][jl] - jc_all[jl]) / jc_all[jl]) if jl.any() else np.zeros(0)
+        # no jet light where the checker has none, and vice versa
+        out["jet_missing"] = int((same & ((jc_all > 0) != (gpu["jet"] > 0))).sum())
+    else:
+        out["jet_rel"] = np.zeros(0)
+        out["jet_missing"] = 0
     steps = same & (wc != abi.HIT_HORIZON)
     out["steps_diff"] = np.abs(gpu["steps"][steps].astype(np.int64) - np.asarray(chk["steps"])[steps])
     return out
@@ -60,7 +69,7 @@ def q(x: np.ndarray, p: float) -> float:
 
 def summary(s: dict) -> str:
     parts = [f"n={s['n']} class_agree={s['class_agree']:.4f}"]
-    for k in ("g_rel", "dir_rad", "Y_rel"):
+    for k in ("g_rel", "dir_rad", "Y_rel", "jet_rel"):
         v = s[k]
         if len(v):
             parts.append(f"{k}: n={len(v)} p50={q(v, .5):.2e} p99={q(v, .99):.2e} max={v.max():.2e}")

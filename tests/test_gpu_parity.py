@@ -57,14 +57,15 @@ def test_fp64_matches_reference_golden(renderer, name):
     msg = summary(s)
     print(name, msg)
     assert s["class_agree"] >= 0.98, msg
-    for k in ("g_rel", "dir_rad", "Y_rel"):
+    assert s["jet_missing"] <= 0.01 * s["n"], msg
+    for k in ("g_rel", "dir_rad", "Y_rel", "jet_rel"):
         assert q(s[k], 0.99) <= FP64_TOL, f"{k}: {msg}"
         # most rays reproduce the reference to rounding
         if len(s[k]) >= 20:
             assert q(s[k], 0.5) <= 1e-9, f"{k}: {msg}"
 
 
-@pytest.mark.parametrize("name", ["a09_i60_centre", "a09_i60_corner", "a0998_i85_ring"])
+@pytest.mark.parametrize("name", ["a09_i60_centre", "a09_i60_corner", "a0998_i85_ring", "quasar_jets", "m87_jets"])
 def test_mixed_meets_accuracy_target_against_reference(renderer, name):
     make, window = CASES[name]
     cfg = make()
@@ -76,7 +77,7 @@ def test_mixed_meets_accuracy_target_against_reference(renderer, name):
     assert s["class_agree"] >= 0.97, msg
     # at least 99% of the rays within the target (all of them when fewer
     # than 100 rays of the kind are in the window)
-    for k, tol in (("g_rel", MIXED_G_TOL), ("dir_rad", MIXED_DIR_TOL)):
+    for k, tol in (("g_rel", MIXED_G_TOL), ("dir_rad", MIXED_DIR_TOL), ("jet_rel", MIXED_G_TOL)):
         v = s[k]
         if len(v) >= 100:
             assert (v <= tol).mean() >= 0.99, msg
@@ -115,7 +116,8 @@ def test_fp64_matches_oracle_on_extension_settings(renderer, orc, sky_mode, stop
     s = compare(gw, chk)
     msg = summary(s)
     assert s["class_agree"] >= 0.98, msg
-    for k in ("g_rel", "dir_rad", "Y_rel"):
+    assert s["jet_missing"] <= 0.01 * s["n"], msg
+    for k in ("g_rel", "dir_rad", "Y_rel", "jet_rel"):
         assert q(s[k], 0.99) <= FP64_TOL, f"{k}: {msg}"
 
 
@@ -179,7 +181,7 @@ def test_content_switches(renderer, orc):
 
 def test_invalid_configs_are_rejected(renderer):
     bad = [
-        dict(width=0), dict(height=-3), dict(jet_enabled=True), dict(precision=7),
+        dict(width=0), dict(height=-3), dict(precision=7),
         dict(sky_mode=9), dict(stop_mode=5), dict(rtol=-1.0), dict(star_count=-1),
     ]
     for kw in bad:
