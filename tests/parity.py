@@ -22,6 +22,12 @@ def window_of(full: np.ndarray, width: int, height: int, spp: int, x0: int, y0: 
     return a[y0:y0 + h, x0:x0 + w].reshape(-1)
 
 
+def _has(x, key: str) -> bool:
+    """Whether a structured array or a mapping (npz) has the field `key`."""
+    names = getattr(getattr(x, "dtype", None), "names", None)
+    return key in names if names is not None else key in x
+
+
 def compare(gpu: np.ndarray, chk: dict) -> dict:
     """Error statistics of GPU samples against checker samples (same order)."""
     wg = gpu["what"].astype(np.int32)
@@ -49,7 +55,7 @@ def compare(gpu: np.ndarray, chk: dict) -> dict:
         out["Y_rel"] = np.abs(gpu["xyz"][lit, 1] - yc) / np.abs(yc)
     else:
         out["Y_rel"] = np.zeros(0)
-    if "jet" in chk and "jet" in gpu.dtype.names:
+    if _has(chk, "jet") and _has(gpu, "jet"):
         jc_all = np.asarray(chk["jet"])
         jl = same & (jc_all > 0)
         out["jet_rel"] = (np.abs(gpu["jet"][jl] - jc_all[jl]) / jc_all[jl]) if jl.any() else np.zeros(0)
