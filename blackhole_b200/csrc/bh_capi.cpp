@@ -729,10 +729,10 @@ static int adjoint_impl(bh_ctx* ctx, const bh_render_config* cfg, const float* t
     return BH_OK;
 }
 
-// The display transform of the frame in ctx->pixels (W x H, device), on
+// The display transform of the W x H frame at d_pixels (device), on
 // ctx->stream; copies the 8-bit image and the exposure back and synchronises.
-static int display_impl(bh_ctx* ctx, const bh_display* d, int width, int height, uint8_t* out_rgb,
-                        double* exposure_used) {
+static int display_impl(bh_ctx* ctx, const bh_display* d, bh_xyz* d_pixels, int width, int height,
+                        uint8_t* out_rgb, double* exposure_used) {
     if (!(d->glare >= 0.0 && d->glare <= 1.0)) return fail(ctx, BH_ERR_INVALID_ARG, "glare must be in [0, 1]");
     if (d->tonemap < BH_TONEMAP_LINEAR || d->tonemap > BH_TONEMAP_HDR)
         return fail(ctx, BH_ERR_INVALID_ARG, "unknown tonemap");
@@ -740,7 +740,7 @@ static int display_impl(bh_ctx* ctx, const bh_display* d, int width, int height,
     int rc;
     DisplayLaunch L;
     std::memset(&L, 0, sizeof L);
-    L.pixels = static_cast<bh_xyz*>(ctx->pixels.p);
+    L.pixels = d_pixels;
     L.width = width;
     L.height = height;
     L.glare = d->glare;
@@ -829,7 +829,7 @@ int bh_gpu_develop(bh_ctx* ctx, const bh_xyz* pixels, int width, int height, con
     if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
     CK(cudaMemcpyAsync(ctx->pixels.p, pixels, npx * sizeof(bh_xyz), cudaMemcpyHostToDevice, ctx->stream));
     ctx->h2d += static_cast<long long>(npx * sizeof(bh_xyz));
-    return display_impl(ctx, d, width, height, out_rgb, exposure_used);
+    return display_impl(ctx, d, static_cast<bh_xyz*>(ctx->pixels.p), width, height, out_rgb, exposure_used);
 }
 
 int bh_gpu_render_rgb(bh_ctx* ctx, const bh_render_config* cfg, const bh_display* d, uint8_t* out_rgb,
@@ -845,9 +845,38 @@ int bh_gpu_render_rgb(bh_ctx* ctx, const bh_render_config* cfg, const bh_display
     if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
     if ((rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true)) != BH_OK)
         return rc;
-    if ((rc = display_impl(ctx, d, cfg->width, cfg->height, out_rgb, exposure_used)) != BH_OK) return rc;
+    if ((rc = display_impl(ctx, d, static_cast<bh_xyz*>(ctx->pixels.p), cfg->width, cfg->height, out_rgb,
+                           exposure_used)) != BH_OK)
+        return rc;
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return finish(ctx, 1, stats, nullptr, true, secs);
+}
+
+int bh_gpu_render_batch_rgb(bh_ctx* ctx, const bh_render_config* cfgs, int n, const bh_display* d,
+                            uint8_t* const* outs_rgb, double* exposure_used, bh_render_stats* stats) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!cfgs || n <= 0 || !outs_rgb || !d) return fail(ctx, BH_ERR_INVALID_ARG, "empty batch");
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device));
+    std::vector<FrameParams> frames;
+    int rc = prepare_frames(ctx, cfgs, n, frames);
+    if (rc != BH_OK) return rc;
+    size_t npx = 0;
+    for (int i = 0; i < n; ++i) npx += static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
+    if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
+    if ((rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true)) != BH_OK)
+        return rc;
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        double e = 0.0;
+        rc = display_impl(ctx, d, static_cast<bh_xyz*>(ctx->pixels.p) + off, cfgs[i].width, cfgs[i].height,
+                          outs_rgb[i], &e);
+        if (rc != BH_OK) return rc;
+        if (exposure_used) exposure_used[i] = e;
+        off += static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
+    }
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return finish(ctx, n, stats, nullptr, true, secs);
 }
 
 int bh_gpu_adjoint(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out) {

@@ -72,6 +72,8 @@ def load_library():
             "bh_gpu_develop": (C.c_int, [ctx_p, P(abi.bh_xyz), C.c_int, C.c_int, P(abi.bh_display),
                                          P(C.c_uint8), P(C.c_double)]),
             "bh_gpu_render_rgb": (C.c_int, [ctx_p, cfg_p, P(abi.bh_display), P(C.c_uint8), P(C.c_double), st_p]),
+            "bh_gpu_render_batch_rgb": (C.c_int, [ctx_p, cfg_p, C.c_int, P(abi.bh_display), P(P(C.c_uint8)),
+                                                  P(C.c_double), st_p]),
             "bh_gpu_adjoint": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4)]),
             "bh_gpu_adjoint_rays": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4), P(C.c_double),
                                               P(C.c_double)]),
@@ -232,6 +234,25 @@ class Renderer:
             stats.update_from(st)
         self._check(rc)
         return out, e.value
+
+    def render_batch_rgb(self, cfgs, display=None, stats: list | None = None, **kw):
+        """Frames of an animation traced in one launch and developed on the
+        device: returns ([rgb uint8 (H, W, 3)], [exposure])."""
+        cs = (abi.bh_render_config * len(cfgs))(*[_as_c(c) for c in cfgs])
+        d = display if display is not None else self.display_settings(**kw)
+        outs = [np.empty((c.height, c.width, 3), dtype=np.uint8) for c in cs]
+        ptrs = (C.POINTER(C.c_uint8) * len(cfgs))(*[o.ctypes.data_as(C.POINTER(C.c_uint8)) for o in outs])
+        ex = (C.c_double * len(cfgs))()
+        sts = (abi.bh_render_stats * len(cfgs))()
+        rc = self.lib.bh_gpu_render_batch_rgb(self._h, cs, len(cfgs), C.byref(d), ptrs, ex, sts)
+        if stats is not None:
+            stats.clear()
+            for st in sts:
+                r = RenderStats()
+                r.update_from(st)
+                stats.append(r)
+        self._check(rc)
+        return outs, list(ex)
 
     # -- discrete adjoint ----------------------------------------------------------
     def adjoint(self, cfg, target, per_ray: bool = False):

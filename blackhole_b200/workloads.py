@@ -196,3 +196,41 @@ def m87_jets(width: int = 320, height: int = 180, precision: int = abi.PRECISION
         quiet=True, precision=precision,
     )
     return _jet_preset(cfg, 130.0, 8.0)
+
+
+def hotspot_orbit(frames: int = 24, width: int = 256, height: int = 144, orbits: float = 1.0,
+                  precision: int = abi.PRECISION_FP64) -> list:
+    """The frames of a hot-spot film as the CLI builds them (main.cpp:78-86,
+    826-835, 950-958): a = 0.9, M = 4.3e6 M_sun, 80 deg from r = 60 M,
+    fov 0.6, disc to 24 M at 0.1 Eddington, a hot spot at r = 8 M
+    (contrast 25, sigma 0.6 M) orbiting progradely; the sequence covers
+    `orbits` orbital periods and frame f sits at u = f / frames of it."""
+    from .config import HotSpot
+
+    base = RenderConfig(
+        M_kg=4.3e6 * M_SUN, spin=0.9,
+        cam=Camera(r=60.0, theta=math.radians(80.0), phi=0.0, fov=0.6),
+        width=width, height=height, sqrt_spp=1, disc_r_out=24.0, eddington=0.1,
+        hotspot=HotSpot(enabled=True, r=8.0, sigma=0.6, contrast=25.0),
+        r_escape=60.0 * 3.0 + 100.0, quiet=True, precision=precision,
+    )
+    base.hotspot.set_spin(base.spin, base.disc_sense)
+    span = orbits * 2.0 * math.pi / abs(base.hotspot.omega)
+    out = []
+    for f in range(frames):
+        c = base.replace()
+        c.observer_time = f / frames * span
+        out.append(c)
+    return out
+
+
+def exposure_probe(cfg: RenderConfig) -> RenderConfig:
+    """The low-resolution probe the CLI meters a film's locked exposure on
+    (main.cpp:931-944), for the frame `cfg` (the sequence's middle frame)."""
+    p = cfg.replace()
+    p.width = max(64, cfg.width // 6)
+    p.height = max(36, cfg.height // 6)
+    p.sqrt_spp = 1
+    p.star_count = min(cfg.star_count, 40000)
+    p.quiet = True
+    return p

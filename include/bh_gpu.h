@@ -417,6 +417,15 @@ int  bh_gpu_develop(bh_ctx* ctx, const bh_xyz* pixels, int width, int height, co
 int  bh_gpu_render_rgb(bh_ctx* ctx, const bh_render_config* cfg, const bh_display* d, uint8_t* out_rgb,
                        double* exposure_used, bh_render_stats* stats);
 
+/* An animation's frames (main.cpp:931-989): all frames traced in one
+   persistent launch, then each one glared and developed on the device into
+   outs_rgb[i] (W_i*H_i*3 bytes, host).  With d->exposure > 0 every frame uses
+   that exposure (the reference locks it from a probe frame, main.cpp:931-944);
+   otherwise each frame is metered on its own.  exposure_used (n doubles) and
+   stats (n entries, as bh_gpu_render_batch) may be NULL. */
+int  bh_gpu_render_batch_rgb(bh_ctx* ctx, const bh_render_config* cfgs, int n, const bh_display* d,
+                             uint8_t* const* outs_rgb, double* exposure_used, bh_render_stats* stats);
+
 /* Measured FMA throughput of `device` in TFLOP/s (2 FLOP per FMA) for
    BH_PRECISION_FP64 (binary64) or BH_PRECISION_MIXED (binary32): the ALU
    roofline of the trace kernel.  Extension; no counterpart in the reference. */
