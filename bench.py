@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--no-photon-ring", action="store_true", help="skip the 4096^2 photon-ring leg")
     p.add_argument("--no-adjoint", action="store_true", help="skip the 512^2 adjoint leg")
     p.add_argument("--no-display", action="store_true", help="skip the on-device display leg")
+    p.add_argument("--no-jets", action="store_true", help="skip the jet and animation legs")
     p.add_argument("--once", action="store_true",
                    help="render the frame once in mixed precision and once in FP64 and exit (for ncu captures)")
     return p.parse_args()
@@ -325,6 +326,51 @@ def batch_leg(r, rank, world, barrier, max_over_ranks, steps=2, warmup=1):
             "steps_per_ray": round(sum(s.steps for s in st) / max(1, sum(s.rays for s in st)), 2)}
 
 
+def jets_leg(r, torch, flush, barrier):
+    """The reference's `quasar` preset with its Blandford-Znajek jets at
+    1024x576: mixed and FP64 device time, rays with jet light, and the mixed
+    path's error in the jet integral against FP64."""
+    from blackhole_b200 import abi, workloads
+
+    cm = workloads.quasar_jets(1024, 576, abi.PRECISION_MIXED)
+    cd = workloads.quasar_jets(1024, 576, abi.PRECISION_FP64)
+    t_m, _, st_m, _ = time_device(r, cm, 2, 1, torch, flush, barrier)
+    t_d, _, st_d, _ = time_device(r, cd, 2, 1, torch, flush, barrier)
+    a = r.trace_rays(cd)
+    b = r.trace_rays(cm)
+    same = (a["what"] == b["what"]) & (a["jet"] > 0)
+    rel = np.abs(b["jet"][same] - a["jet"][same]) / a["jet"][same]
+    return {"workload": "quasar_jets: reference `quasar` preset (a=0.998, 84 deg, r_cam 80 M, fov 0.90, "
+                        "disc to 20 M at 0.5 Eddington, jets to z=130 M, Gamma_max 10), 1024x576, 1 spp",
+            "rays": cm.n_rays,
+            "mixed": {"value": round(cm.n_rays * 2 / (t_m * 1e-3), 1), "unit": "rays/s", "ms": round(t_m / 2, 3),
+                      "jet_rays": st_m.jet_rays, "steps_per_ray": round(st_m.steps / st_m.rays, 2)},
+            "fp64": {"value": round(cd.n_rays * 2 / (t_d * 1e-3), 1), "unit": "rays/s", "ms": round(t_d / 2, 3),
+                     "jet_rays": st_d.jet_rays, "steps_per_ray": round(st_d.steps / st_d.rays, 2)},
+            "mixed_jet_rel_err": {"p50": float(np.quantile(rel, .5)), "p99": float(np.quantile(rel, .99)),
+                                  "max": float(rel.max()), "n": int(same.sum())} if same.any() else None}
+
+
+def animation_leg(r, frames=48, width=512, height=288):
+    """A hot-spot film made the CLI's way: exposure metered on a probe of the
+    middle frame, then all frames traced in one launch and developed on the
+    device (bh_gpu_render_batch_rgb); wall clock from the configs to the
+    8-bit frames in host memory."""
+    from blackhole_b200 import workloads
+
+    film = workloads.hotspot_orbit(frames=frames, width=width, height=height)
+    r.render_batch_rgb(film[:2], exposure=1.0)             # warm-up
+    t0 = time.perf_counter()
+    _, e = r.render_rgb(workloads.exposure_probe(film[len(film) // 2]), meter_only=True)
+    _, used = r.render_batch_rgb(film, exposure=e)
+    wall = time.perf_counter() - t0
+    rays = sum(c.n_rays for c in film)
+    return {"workload": f"hotspot_orbit: {frames} frames {width}x{height}, a=0.9, 80 deg, r_cam 60 M, hot spot "
+                        "at 8 M over one orbit, HDR curve, exposure locked from a probe",
+            "value": round(frames / wall, 2), "unit": "frames/s", "rays_per_s": round(rays / wall, 1),
+            "seconds": round(wall, 3), "exposure": e}
+
+
 def adjoint_leg(r, steps=3, warmup=1):
     """Gradients per second of the discrete adjoint on the 512^2 gradient
     workload: one gradient = the binary64 render, the loss against the target
@@ -478,6 +524,16 @@ def gpu_arm(args):
     # binary64 resume trace, shade, 2 reduce.
     out["gpu_launches"] = 5 * args.steps
     out["clocks"] = clk.summary()
+
+    if not args.no_jets:
+        try:
+            out["jets"] = jets_leg(r, torch, flush, barrier)
+        except Exception as e:  # reported, not hidden
+            out["jets"] = {"error": repr(e)}
+        try:
+            out["animation"] = animation_leg(r)
+        except Exception as e:  # reported, not hidden
+            out["animation"] = {"error": repr(e)}
 
     if not args.no_adjoint:
         try:
