@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true", help="skip the 512^2 adjoint leg")
     p.add_argument("--no-display", action="store_true", help="skip the on-device display leg")
     p.add_argument("--no-jets", action="store_true", help="skip the jet and animation legs")
+    p.add_argument("--leg", default=None, choices=["adjoint", "display", "jets"],
+                   help="run one workload once (for profiling) and exit")
     p.add_argument("--once", action="store_true",
                    help="render the frame once in mixed precision and once in FP64 and exit (for ncu captures)")
     return p.parse_args()
@@ -636,9 +638,41 @@ def once(args):
                               "attempts": st.attempts, "rays": st.rays}), flush=True)
 
 
+def leg_once(args):
+    """One invocation of one workload, for a profiler's launch list or a
+    single-kernel capture: `adjoint` (bh_gpu_adjoint at --size^2 on the
+    gradient workload), `display` (bh_gpu_develop of the --size^2 edge-on
+    frame, HDR, metered), `jets` (the quasar preset at --size x 9/16 --size,
+    mixed then FP64)."""
+    from blackhole_b200 import Renderer, RenderStats, abi, workloads
+
+    with Renderer(0) as r:
+        if args.leg == "adjoint":
+            cfg = workloads.adjoint_512()
+            cfg.width = cfg.height = args.size
+            t = workloads.adjoint_512(target=True)
+            t.width = t.height = args.size
+            target = r.render(t)[..., 1].astype(np.float32)
+            g = r.adjoint(cfg, target)
+            print(json.dumps({k: g[k] for k in ("loss", "d_spin", "kernel_ms", "steps", "replayed_steps")}))
+        elif args.leg == "display":
+            xyz = r.render(frame_config(args.size, 0, 1, abi.PRECISION_MIXED))
+            rgb, e = r.develop(xyz, glare=0.3)
+            print(json.dumps({"exposure": e, "mean": float(rgb.mean())}))
+        elif args.leg == "jets":
+            for prec in (abi.PRECISION_MIXED, abi.PRECISION_FP64):
+                st = RenderStats()
+                r.render(workloads.quasar_jets(args.size, args.size * 9 // 16, prec), st)
+                print(json.dumps({"precision": prec, "kernel_ms": st.kernel_ms, "jet_rays": st.jet_rays}))
+        else:
+            raise SystemExit(f"unknown leg {args.leg!r}")
+
+
 def main():
     args = parse()
-    if args.once:
+    if args.leg:
+        leg_once(args)
+    elif args.once:
         once(args)
     elif args.impl == "reference":
         reference_arm(args)
