@@ -291,12 +291,13 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     tl.budget = ctx->budget;
     tl.deferred = p.mixed ? ctx->deferred.p : nullptr;
     tl.reg_variant = (lp.reg_variant == 2) ? 1 : 0;
-    // The binary64 pass that finishes deferred mixed-precision rays runs with
-    // the FP64 launch shape.
-    tl.block_resume = lp64.block_size;
-    tl.reg_variant_resume = (lp64.reg_variant == 2) ? 1 : 0;
+    // The binary64 pass that finishes deferred mixed-precision rays: few rays
+    // with long serial step chains, so it runs the spill-free (wide) register
+    // variant in small blocks.
+    tl.block_resume = 64;
+    tl.reg_variant_resume = 1;
     {
-        int bps64 = trace_blocks_per_sm(BH_PRECISION_FP64, lp64.block_size, lp64.reg_variant == 2);
+        int bps64 = trace_blocks_per_sm(BH_PRECISION_FP64, tl.block_resume, true);
         tl.grid_resume = ctx->sm_count * (bps64 < 1 ? 1 : bps64);
     }
     tl.resume_event = timed ? ctx->ev[3] : nullptr;
