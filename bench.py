@@ -403,6 +403,27 @@ def adjoint_leg(r, steps=3, warmup=1):
             "disc_rays": gs["disc_rays"], "sky_rays": gs["sky_rays"]}
 
 
+def ring_adjoint_leg(r, steps=2):
+    """Gradients per second with respect to (spin, inclination) on the
+    1024^2 central crop of the photon-ring frame (binary64), against the
+    crop rendered at a = 0.99, 76 deg."""
+    from blackhole_b200 import workloads
+
+    cfg = workloads.photon_ring_crop(1024)
+    target = r.render(workloads.photon_ring_crop(1024, target=True))[..., 1].astype(np.float32)
+    r.adjoint(cfg, target)
+    ms, g = [], None
+    for _ in range(steps):
+        g = r.adjoint(cfg, target)
+        ms.append(g["kernel_ms"])
+    m = sum(ms) / len(ms)
+    return {"workload": "photon_ring_crop: central 1024^2 of the photon-ring frame (a=0.998, 75 deg, "
+                        "critical-curve centre), binary64; target at a=0.99, 76 deg",
+            "value": round(1e3 / m, 2), "unit": "grads/s", "ms_per_grad": round(m, 3),
+            "grad": [g["d_spin"], g["d_inclination"]], "loss": g["loss"],
+            "steps_per_ray": round(g["steps"] / g["rays"], 2)}
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -542,6 +563,10 @@ def gpu_arm(args):
             out["adjoint"] = adjoint_leg(r)
         except Exception as e:  # reported, not hidden
             out["adjoint"] = {"error": repr(e)}
+        try:
+            out["photon_ring_adjoint"] = ring_adjoint_leg(r)
+        except Exception as e:  # reported, not hidden
+            out["photon_ring_adjoint"] = {"error": repr(e)}
 
     if not args.no_photon_ring:
         try:

@@ -157,6 +157,20 @@ def photon_ring_4096(precision: int = abi.PRECISION_MIXED, size: int = 4096) -> 
     return cfg
 
 
+def photon_ring_crop(size: int = 1024, target: bool = False) -> RenderConfig:
+    """The central size x size crop of the 4096^2 photon-ring frame (same
+    pixel scale, same centre on the critical curve), in binary64, for the
+    adjoint with respect to spin and inclination.  target: the frame at
+    a = 0.99, inclination 76 deg the loss is measured against."""
+    cfg = photon_ring_4096(abi.PRECISION_FP64)
+    cfg.cam.fov = 2.0 * math.atan(math.tan(0.5 * cfg.cam.fov) * size / 4096.0)
+    cfg.width = cfg.height = size
+    if target:
+        cfg.spin = 0.99
+        cfg.cam.theta = math.radians(76.0)
+    return cfg
+
+
 def _jet_preset(cfg: RenderConfig, z_top: float, gamma_max: float) -> RenderConfig:
     """Jets on, configured the way the CLI does (main.cpp:399-423), and the
     escape sphere outside them (main.cpp:881-890)."""
