@@ -115,37 +115,53 @@ __global__ void exposure_hist(const bh_xyz* __restrict__ px, long long n, Exposu
     }
 }
 
-// Pick the digit holding each target's order statistic; after the last
-// (least significant) digit, form the exposure.
-__global__ void exposure_pick(ExposureState* st, int shift, int first, int last, double key,
-                              double fixed, double* exposure) {
-    if (threadIdx.x != 0) return;
+// Pick the digit holding each target's order statistic: one thread per digit,
+// a block-wide inclusive scan of the counts, and the thread whose range holds
+// the rank extends the prefix.  After the last (least significant) digit,
+// form the exposure.
+constexpr int kPickThreads = 256;
+
+__global__ void __launch_bounds__(kPickThreads)
+exposure_pick(ExposureState* st, int shift, int first, int last, double key, double fixed, double* exposure) {
+    __shared__ unsigned long long scan[2][kPickThreads];
+    const int d = threadIdx.x;
     const unsigned long long m = st->count;
-    if (first && m > 0) {
-        const double q[2] = {0.999, 0.9999};
-        for (int t = 0; t < 2; ++t) {
-            unsigned long long k = (unsigned long long)(q[t] * (double)(m - 1));
-            st->k[t] = (k > m - 1) ? m - 1 : k;
-        }
+    if (first && m > 0 && d < 2) {
+        const double q = (d == 0) ? 0.999 : 0.9999;
+        const unsigned long long k = (unsigned long long)(q * (double)(m - 1));
+        st->k[d] = (k > m - 1) ? m - 1 : k;
     }
+    __syncthreads();
+    const unsigned long long c0 = st->hist[0][d], c1 = st->hist[1][d];
+    scan[0][d] = c0;
+    scan[1][d] = c1;
+    __syncthreads();
+    for (int off = 1; off < kPickThreads; off <<= 1) {
+        const unsigned long long a0 = (d >= off) ? scan[0][d - off] : 0ull;
+        const unsigned long long a1 = (d >= off) ? scan[1][d - off] : 0ull;
+        __syncthreads();
+        scan[0][d] += a0;
+        scan[1][d] += a1;
+        __syncthreads();
+    }
+    const unsigned long long k0 = st->k[0], k1 = st->k[1];
+    __syncthreads();
     if (m > 0) {
-        for (int t = 0; t < 2; ++t) {
-            unsigned long long cum = 0;
-            for (int d = 0; d < 256; ++d) {
-                const unsigned long long c = st->hist[t][d];
-                if (st->k[t] < cum + c) {
-                    st->prefix[t] |= (unsigned long long)d << shift;
-                    st->k[t] -= cum;
-                    break;
-                }
-                cum += c;
-            }
+        const unsigned long long e0 = scan[0][d] - c0, e1 = scan[1][d] - c1;   // counts below digit d
+        if (c0 && k0 >= e0 && k0 < e0 + c0) {
+            st->prefix[0] |= (unsigned long long)d << shift;
+            st->k[0] = k0 - e0;
         }
-        st->mask |= 255ull << shift;
+        if (c1 && k1 >= e1 && k1 < e1 + c1) {
+            st->prefix[1] |= (unsigned long long)d << shift;
+            st->k[1] = k1 - e1;
+        }
+        if (d == 0) st->mask |= 255ull << shift;
     }
-    for (int t = 0; t < 2; ++t)
-        for (int d = 0; d < 256; ++d) st->hist[t][d] = 0ull;
-    if (last) {
+    st->hist[0][d] = 0ull;
+    st->hist[1][d] = 0ull;
+    __syncthreads();
+    if (last && d == 0) {
         double e = fixed;
         if (!(fixed > 0.0)) {
             e = 1.0;
@@ -240,10 +256,11 @@ cudaError_t launch_display(const DisplayLaunch& L, cudaStream_t s) {
         for (int pass = 0; pass < 8; ++pass) {
             const int shift = 56 - 8 * pass;
             exposure_hist<<<grid, kThreads, 0, s>>>(L.pixels, n, L.state, shift);
-            exposure_pick<<<1, 32, 0, s>>>(L.state, shift, pass == 0, pass == 7, L.key, 0.0, L.exposure_out);
+            exposure_pick<<<1, kPickThreads, 0, s>>>(L.state, shift, pass == 0, pass == 7, L.key, 0.0,
+                                                     L.exposure_out);
         }
     } else {
-        exposure_pick<<<1, 32, 0, s>>>(L.state, 0, 0, 1, L.key, L.exposure, L.exposure_out);
+        exposure_pick<<<1, kPickThreads, 0, s>>>(L.state, 0, 0, 1, L.key, L.exposure, L.exposure_out);
     }
     if (L.rgb)
         develop_kernel<<<blocks, kThreads, 0, s>>>(L.pixels, n, L.exposure_out, L.tonemap, L.log_k, L.denom, L.rgb);
