@@ -200,7 +200,22 @@ def roofline(kernel_ms: float, steps: int, attempts: int, precision: str, peak: 
         "accepted_steps": steps,
         "attempts": attempts,
         "kernel_ms": round(kernel_ms, 4),
+        # The HBM side of the same launch: the measured DRAM bytes against the
+        # measured copy bandwidth (the path is not memory-bound).
+        "hbm": hbm_side(traffic, kernel_ms),
     }
+
+
+def hbm_side(traffic, kernel_ms):
+    if traffic is None or not os.path.exists(MEASURED_PEAKS):
+        return None
+    try:
+        peak = float(json.load(open(MEASURED_PEAKS))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return None
+    gbs = traffic / (kernel_ms * 1e-3) / 1e9
+    return {"achieved": round(gbs, 2), "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 5),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
 
 
 def accuracy(r, size, rank, world, cfgs=None):
