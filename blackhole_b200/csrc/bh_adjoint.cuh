@@ -117,17 +117,17 @@ struct RayC {
 // Hamilton's equations in Carter's separated form (the render path's
 // right-hand side, geodesic.h:50-71):
 //   2 Sigma H = Delta p_r^2 + p_th^2 + (L_z - a E sin^2)^2 / sin^2
-//               - ((r^2 + a^2) E - a L_z)^2 / Delta.
-// d = (dt, dr, dth, dphi, dp_r, dp_th) / dlambda; *cs_out = cos(th).
-__host__ __device__ BHA_NOINLINE void rhs6(const RayC& c, double r, double th, double pr, double pth,
-                                           double d[6], double* cs_out) {
-    double sn, cs;
-    sc(th, &sn, &cs);
+//               - ((r^2 + a^2) E - a L_z)^2 / Delta,
+// at sin(th) = sn, cos(th) = cs, with one reciprocal (of Sigma Delta sin^2)
+// for the three quotients.  d = (dt, dr, dth, dphi, dp_r, dp_th) / dlambda.
+__host__ __device__ BHA_NOINLINE void rhs6(const RayC& c, double r, double sn, double cs, double pr, double pth,
+                                           double d[6]) {
     if (fabs(sn) < 1e-9) sn = (sn < 0.0) ? -1e-9 : 1e-9;   // kerr.h:51
     const double sn2 = sn * sn, cs2 = cs * cs, r2 = r * r;
     const double S = r2 + c.a2 * cs2;
     const double D = c.factored ? (r - c.rp) * (r - c.rm) : (r2 - 2.0 * r + c.a2);
-    const double iS = 1.0 / S, iD = 1.0 / D, isn2 = 1.0 / sn2;
+    const double inv = 1.0 / (S * D * sn2);
+    const double iS = inv * D * sn2, iD = inv * S * sn2, isn2 = inv * S * D;
     const double r2a2 = r2 + c.a2;
     const double K = r2a2 * c.E - c.a * c.Lz;
     const double Lp = c.Lz - c.a * c.E * sn2;
@@ -140,17 +140,25 @@ __host__ __device__ BHA_NOINLINE void rhs6(const RayC& c, double r, double th, d
     d[3] = iS * (Lp * isn2 + c.a * KiD);
     d[4] = -0.5 * iS * (Dr * pr * pr - 4.0 * r * c.E * KiD + Dr * KiD * KiD - 2.0 * r * B * iS);
     d[5] = -sn * cs * iS * (c.a2 * c.E * c.E - c.Lz * c.Lz * isn2 * isn2 + c.a2 * B * iS);
+}
+
+// The right-hand side at angle th; *sn_out, *cs_out receive sin(th), cos(th).
+__host__ __device__ __forceinline__ void rhs6_th(const RayC& c, double r, double th, double pr, double pth,
+                                                 double d[6], double* sn_out, double* cs_out) {
+    double sn, cs;
+    sc(th, &sn, &cs);
+    rhs6(c, r, sn, cs, pr, pth, d);
+    *sn_out = sn;
     *cs_out = cs;
 }
 
-// Vector-Jacobian product of rhs6: given db = dLoss/d(d), adds dLoss/d(r, th,
-// p_r, p_th) into g[0..3] and dLoss/d(E, L_z, a) into *Eb, *Lzb, *ab.
-// Reverse-mode differentiation of the expressions of rhs6, written out.
-__host__ __device__ BHA_NOINLINE void rhs6_vjp(const RayC& c, double r, double th, double pr, double pth,
+// Vector-Jacobian product of rhs6 at (r, th, p_r, p_th) given sin(th) = sn
+// and cos(th) = cs: for db = dLoss/d(d), adds dLoss/d(r, th, p_r, p_th) into
+// g[0..3] and dLoss/d(E, L_z, a) into *Eb, *Lzb, *ab.  Reverse-mode
+// differentiation of the expressions of rhs6, written out.
+__host__ __device__ BHA_NOINLINE void rhs6_vjp(const RayC& c, double r, double sn, double cs, double pr, double pth,
                                                const double db[6], double g[4], double* Eb, double* Lzb,
                                                double* ab) {
-    double sn, cs;
-    sc(th, &sn, &cs);
     const double sn_true = sn;
     const bool clamped = fabs(sn) < 1e-9;
     if (clamped) sn = (sn < 0.0) ? -1e-9 : 1e-9;
@@ -158,7 +166,8 @@ __host__ __device__ BHA_NOINLINE void rhs6_vjp(const RayC& c, double r, double t
     const double sn2 = sn * sn, cs2 = cs * cs, r2 = r * r;
     const double S = r2 + a2 * cs2;
     const double D = c.factored ? (r - c.rp) * (r - c.rm) : (r2 - 2.0 * r + a2);
-    const double iS = 1.0 / S, iD = 1.0 / D, isn2 = 1.0 / sn2;
+    const double inv = 1.0 / (S * D * sn2);
+    const double iS = inv * D * sn2, iD = inv * S * sn2, isn2 = inv * S * D;
     const double r2a2 = r2 + a2;
     const double K = r2a2 * E - a * Lz;
     const double Lp = Lz - a * E * sn2;
@@ -291,7 +300,8 @@ __host__ __device__ BHA_NOINLINE bool advance(const FrameParams& F, const RayC& 
                                 {A51, A52, A53, A54, 0},
                                 {A61, A62, A63, A64, A65}};
     if (!s.have_k1) {
-        rhs6(c, s.y[1], s.y[2], s.y[4], s.y[5], s.k1, &s.c0);
+        double sn0;
+        rhs6_th(c, s.y[1], s.y[2], s.y[4], s.y[5], s.k1, &sn0, &s.c0);
         s.have_k1 = 1;
     }
     for (;;) {
@@ -300,7 +310,7 @@ __host__ __device__ BHA_NOINLINE bool advance(const FrameParams& F, const RayC& 
             if (s.h > hmax) s.h = hmax;
         }
         const double h = s.h;
-        double k[7][6], t[6], yn[6], c7, cs;
+        double k[7][6], t[6], yn[6], c7, sn, cs;
         for (int i = 0; i < 6; ++i) k[0][i] = s.k1[i];
         #pragma unroll
         for (int j = 1; j < 6; ++j) {
@@ -311,11 +321,11 @@ __host__ __device__ BHA_NOINLINE bool advance(const FrameParams& F, const RayC& 
                 for (int l = 0; l < j; ++l) acc += A[j][l] * k[l][i];
                 t[i] = s.y[i] + h * acc;
             }
-            rhs6(c, t[1], t[2], t[4], t[5], k[j], &cs);
+            rhs6_th(c, t[1], t[2], t[4], t[5], k[j], &sn, &cs);
         }
         for (int i = 0; i < 6; ++i)
             yn[i] = s.y[i] + h * (B1 * k[0][i] + B3 * k[2][i] + B4 * k[3][i] + B5 * k[4][i] + B6 * k[5][i]);
-        rhs6(c, yn[1], yn[2], yn[4], yn[5], k[6], &c7);
+        rhs6_th(c, yn[1], yn[2], yn[4], yn[5], k[6], &sn, &c7);
         double err2 = 0.0;
         for (int i = 0; i < 6; ++i) {
             const double e = h * (E1 * k[0][i] + E3 * k[2][i] + E4 * k[3][i] + E5 * k[4][i] + E6 * k[5][i] +
@@ -405,9 +415,11 @@ __host__ __device__ BHA_NOINLINE void step_vjp(const RayC& c, const double ys[6]
                                 {A41, A42, A43, 0, 0},
                                 {A51, A52, A53, A54, 0},
                                 {A61, A62, A63, A64, A65}};
-    double k[7][6], Y[6][4], t[6], yn[6], cs;
+    // Stage inputs (r, th, p_r, p_th) and the sine and cosine of their th,
+    // kept for the stages' vector-Jacobian products.
+    double k[7][6], Y[6][4], Ysn[6], Ycs[6], t[6], yn[6];
     Y[0][0] = ys[1]; Y[0][1] = ys[2]; Y[0][2] = ys[4]; Y[0][3] = ys[5];
-    rhs6(c, ys[1], ys[2], ys[4], ys[5], k[0], &cs);
+    rhs6_th(c, ys[1], ys[2], ys[4], ys[5], k[0], &Ysn[0], &Ycs[0]);
     #pragma unroll
     for (int j = 1; j < 6; ++j) {
         #pragma unroll
@@ -418,7 +430,7 @@ __host__ __device__ BHA_NOINLINE void step_vjp(const RayC& c, const double ys[6]
             t[i] = ys[i] + h * acc;
         }
         Y[j][0] = t[1]; Y[j][1] = t[2]; Y[j][2] = t[4]; Y[j][3] = t[5];
-        rhs6(c, t[1], t[2], t[4], t[5], k[j], &cs);
+        rhs6_th(c, t[1], t[2], t[4], t[5], k[j], &Ysn[j], &Ycs[j]);
     }
     for (int i = 0; i < 6; ++i)
         yn[i] = ys[i] + h * (B1 * k[0][i] + B3 * k[2][i] + B4 * k[3][i] + B5 * k[4][i] + B6 * k[5][i]);
@@ -431,7 +443,8 @@ __host__ __device__ BHA_NOINLINE void step_vjp(const RayC& c, const double ys[6]
         ybar[i] = 0.0;
     }
     if (rstar_b != 0.0) {
-        rhs6(c, yn[1], yn[2], yn[4], yn[5], k[6], &cs);
+        double sn7, cs7;
+        rhs6_th(c, yn[1], yn[2], yn[4], yn[5], k[6], &sn7, &cs7);
         const DenseC cth = dense_coef(h, ys[2], yn[2], k[0][2], k[2][2], k[3][2], k[4][2], k[5][2], k[6][2]);
         const DenseC crr = dense_coef(h, ys[1], yn[1], k[0][1], k[2][1], k[3][1], k[4][1], k[5][1], k[6][1]);
         const double target = crossing_target(cth.r1, cth.r1 + cth.r2);
@@ -440,7 +453,7 @@ __host__ __device__ BHA_NOINLINE void step_vjp(const RayC& c, const double ys[6]
         dense_vjp(h, s, rstar_b, 1, ybar, ynb, kb);
         if (dth != 0.0) dense_vjp(h, s, -rstar_b * dr / dth, 2, ybar, ynb, kb);
         double g4[4] = {0.0, 0.0, 0.0, 0.0};
-        rhs6_vjp(c, yn[1], yn[2], yn[4], yn[5], kb[6], g4, Eb, Lzb, ab);
+        rhs6_vjp(c, yn[1], sn7, cs7, yn[4], yn[5], kb[6], g4, Eb, Lzb, ab);
         ynb[1] += g4[0]; ynb[2] += g4[1]; ynb[4] += g4[2]; ynb[5] += g4[3];
     }
     for (int i = 0; i < 6; ++i) {
@@ -454,7 +467,7 @@ __host__ __device__ BHA_NOINLINE void step_vjp(const RayC& c, const double ys[6]
     #pragma unroll
     for (int j = 5; j >= 0; --j) {
         double g4[4] = {0.0, 0.0, 0.0, 0.0};
-        rhs6_vjp(c, Y[j][0], Y[j][1], Y[j][2], Y[j][3], kb[j], g4, Eb, Lzb, ab);
+        rhs6_vjp(c, Y[j][0], Ysn[j], Ycs[j], Y[j][2], Y[j][3], kb[j], g4, Eb, Lzb, ab);
         const double Yb[6] = {0.0, g4[0], g4[1], 0.0, g4[2], g4[3]};
         #pragma unroll
         for (int i = 0; i < 6; ++i) {

@@ -7,6 +7,7 @@
 // the render library and never loaded by it.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -80,8 +81,8 @@ extern "C" {
 
 // Right-hand side at (r, th, p_r, p_th) for constants (a, a^2, E, L_z, r+, r-, factored).
 int bhx_rhs(const double c7[7], const double x4[4], double d[6]) {
-    double cs;
-    adj::rhs6(ray_consts(c7), x4[0], x4[1], x4[2], x4[3], d, &cs);
+    double sn, cs;
+    adj::rhs6_th(ray_consts(c7), x4[0], x4[1], x4[2], x4[3], d, &sn, &cs);
     return 0;
 }
 
@@ -89,7 +90,7 @@ int bhx_rhs(const double c7[7], const double x4[4], double d[6]) {
 int bhx_rhs_vjp(const double c7[7], const double x4[4], const double db[6], double out[7]) {
     double g[4] = {0, 0, 0, 0};
     double Eb = 0, Lzb = 0, ab = 0;
-    adj::rhs6_vjp(ray_consts(c7), x4[0], x4[1], x4[2], x4[3], db, g, &Eb, &Lzb, &ab);
+    adj::rhs6_vjp(ray_consts(c7), x4[0], std::sin(x4[1]), std::cos(x4[1]), x4[2], x4[3], db, g, &Eb, &Lzb, &ab);
     for (int i = 0; i < 4; ++i) out[i] = g[i];
     out[4] = Eb;
     out[5] = Lzb;
