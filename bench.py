@@ -439,6 +439,27 @@ def ring_adjoint_leg(r, steps=2):
             "steps_per_ray": round(g["steps"] / g["rays"], 2)}
 
 
+def autotune_leg():
+    """The launch-shape autotuner on the 64-frame batch: the search runs on
+    every fourth frame of it (16 frames), then the whole batch is timed with
+    the shape it keeps.  A fresh context, so no other leg sees the shape."""
+    from blackhole_b200 import Renderer, workloads
+
+    frames = workloads.batch_64_frames()
+    with Renderer(0) as r:
+        default = r.get_launch(frames[0].precision)
+        r.render_batch(frames[::4])
+        best, ms = r.autotune_batch(frames[::4])
+        st = []
+        r.render_batch(frames, st)
+        r.render_batch(frames, st)
+        rays = sum(c.n_rays for c in frames)
+        return {"searched_on": "every 4th frame of batch_64_frames (16 frames)", "default": default,
+                "best": best, "best_ms_on_subset": round(ms, 3),
+                "batch_with_best": {"value": round(rays / (st[0].kernel_ms * 1e-3), 1), "unit": "rays/s",
+                                    "ms": round(st[0].kernel_ms, 3)}}
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -594,6 +615,11 @@ def gpu_arm(args):
             out["batch"] = batch_leg(r, rank, world, barrier, max_over_ranks)
         except Exception as e:  # reported, not hidden
             out["batch"] = {"error": repr(e)}
+        if world == 1:
+            try:
+                out["autotune"] = autotune_leg()
+            except Exception as e:  # reported, not hidden
+                out["autotune"] = {"error": repr(e)}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -937,34 +937,49 @@ int bh_gpu_get_launch(const bh_ctx* ctx, int precision, bh_launch_params* p) {
     return BH_OK;
 }
 
-int bh_gpu_autotune(bh_ctx* ctx, const bh_render_config* cfg, bh_launch_params* best, double* best_ms) {
-    if (!ctx || !cfg) return BH_ERR_INVALID_ARG;
-    int rc = check_cfg_header(ctx, cfg);
+// The launch-shape search of bh_gpu_autotune / bh_gpu_autotune_batch: every
+// shape of the space renders the frame(s) twice, the shorter trace time
+// counts, and the fastest shape is kept for cfgs[0].precision.
+static int autotune_impl(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_launch_params* best,
+                         double* best_ms) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!cfgs || n <= 0) return fail(ctx, BH_ERR_INVALID_ARG, "no frames to tune on");
+    int rc = check_cfg_header(ctx, &cfgs[0]);
     if (rc != BH_OK) return rc;
-    const int prec = cfg->precision;
+    const int prec = cfgs[0].precision;
     if (prec != BH_PRECISION_FP64 && prec != BH_PRECISION_MIXED)
         return fail(ctx, BH_ERR_INVALID_ARG, "unknown precision");
     const int slot = prec == BH_PRECISION_MIXED ? 1 : 0;
     const bh_launch_params keep = ctx->launch[slot];
-    std::vector<bh_xyz> px(static_cast<size_t>(std::max(cfg->width, 1)) * std::max(cfg->height, 1));
+    std::vector<std::vector<bh_xyz>> px(n);
+    std::vector<bh_xyz*> outs(n);
+    for (int i = 0; i < n; ++i) {
+        px[i].resize(static_cast<size_t>(std::max(cfgs[i].width, 1)) * std::max(cfgs[i].height, 1));
+        outs[i] = px[i].data();
+    }
+    std::vector<bh_render_stats> st(n);
     bh_launch_params winner = keep;
     double winner_ms = 1e300;
     for (int rv = 1; rv <= 2; ++rv)
         for (int bs : {64, 128, 256, 512})
-            for (int rpt : {1, 2, 4})
+            for (int rpt : {1, 2, 4, 8})
                 for (int refill : {8, 16, 24, 32}) {
                     if (bs * trace_registers(prec, rv == 2) > 65536) continue;
-                    bh_launch_params p{bs, rpt, refill, 0, rv};
+                    const bh_launch_params p{bs, rpt, refill, 0, rv};
                     ctx->launch[slot] = p;
-                    bh_render_stats st;
-                    std::memset(&st, 0, sizeof st);
-                    rc = bh_gpu_render(ctx, cfg, px.data(), &st);
-                    if (rc != BH_OK) {
-                        ctx->launch[slot] = keep;
-                        return rc;
+                    double ms = 1e300;
+                    for (int rep = 0; rep < 2; ++rep) {
+                        std::memset(st.data(), 0, n * sizeof(bh_render_stats));
+                        rc = (n == 1) ? bh_gpu_render(ctx, &cfgs[0], outs[0], st.data())
+                                      : bh_gpu_render_batch(ctx, cfgs, n, outs.data(), st.data());
+                        if (rc != BH_OK) {
+                            ctx->launch[slot] = keep;
+                            return rc;
+                        }
+                        ms = std::min(ms, st[0].kernel_ms);
                     }
-                    if (st.kernel_ms < winner_ms) {
-                        winner_ms = st.kernel_ms;
+                    if (ms < winner_ms) {
+                        winner_ms = ms;
                         winner = p;
                     }
                 }
@@ -972,6 +987,15 @@ int bh_gpu_autotune(bh_ctx* ctx, const bh_render_config* cfg, bh_launch_params* 
     if (best) *best = winner;
     if (best_ms) *best_ms = winner_ms;
     return BH_OK;
+}
+
+int bh_gpu_autotune(bh_ctx* ctx, const bh_render_config* cfg, bh_launch_params* best, double* best_ms) {
+    return autotune_impl(ctx, cfg, 1, best, best_ms);
+}
+
+int bh_gpu_autotune_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_launch_params* best,
+                          double* best_ms) {
+    return autotune_impl(ctx, cfgs, n, best, best_ms);
 }
 
 int bh_gpu_set_step_budget(bh_ctx* ctx, long long budget) {

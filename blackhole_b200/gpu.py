@@ -59,6 +59,7 @@ def load_library():
             "bh_gpu_set_launch": (C.c_int, [ctx_p, C.c_int, P(abi.bh_launch_params)]),
             "bh_gpu_get_launch": (C.c_int, [ctx_p, C.c_int, P(abi.bh_launch_params)]),
             "bh_gpu_autotune": (C.c_int, [ctx_p, cfg_p, P(abi.bh_launch_params), P(C.c_double)]),
+            "bh_gpu_autotune_batch": (C.c_int, [ctx_p, cfg_p, C.c_int, P(abi.bh_launch_params), P(C.c_double)]),
             "bh_gpu_set_step_budget": (C.c_int, [ctx_p, C.c_longlong]),
             "bh_gpu_request_abort": (None, [ctx_p]),
             "bh_gpu_clear_abort": (None, [ctx_p]),
@@ -297,6 +298,14 @@ class Renderer:
         p = abi.bh_launch_params()
         ms = C.c_double(0.0)
         self._check(self.lib.bh_gpu_autotune(self._h, C.byref(c), C.byref(p), C.byref(ms)))
+        return {k: getattr(p, k) for k, _ in p._fields_}, ms.value
+
+    def autotune_batch(self, cfgs) -> tuple:
+        """The launch-shape search on a batch of frames; keeps and returns (best, ms)."""
+        cs = (abi.bh_render_config * len(cfgs))(*[_as_c(c) for c in cfgs])
+        p = abi.bh_launch_params()
+        ms = C.c_double(0.0)
+        self._check(self.lib.bh_gpu_autotune_batch(self._h, cs, len(cfgs), C.byref(p), C.byref(ms)))
         return {k: getattr(p, k) for k, _ in p._fields_}, ms.value
 
     def set_step_budget(self, budget: int) -> None:

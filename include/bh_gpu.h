@@ -281,12 +281,21 @@ int  bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n,
 int  bh_gpu_set_launch(bh_ctx* ctx, int precision, const bh_launch_params* p);
 int  bh_gpu_get_launch(const bh_ctx* ctx, int precision, bh_launch_params* p);
 
-/* Autotuner: render `cfg` once per launch shape of the search space (block
-   size 64..512, rays per thread 1..4, refill threshold 8..32 idle lanes,
+/* Autotuner: render `cfg` twice per launch shape of the search space (block
+   size 64..512, rays per thread 1..8, refill threshold 8..32 idle lanes,
    both register caps), keep the shape with the shortest trace-kernel time for
    cfg->precision, and return it in *best (and its time in *best_ms).  Extension;
    no counterpart in the reference. */
 int  bh_gpu_autotune(bh_ctx* ctx, const bh_render_config* cfg, bh_launch_params* best, double* best_ms);
+
+/* The same search on a batch of frames through bh_gpu_render_batch (each
+   shape timed on the captured batch graph; *best_ms is its device time).
+   The search space: block size 64..512, rays per thread 1..8, refill
+   threshold 8..32 idle lanes (a refill claims n_idle x rays_per_thread rays,
+   8 to 256, in one atomic), both register caps.  Extension; no counterpart
+   in the reference. */
+int  bh_gpu_autotune_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_launch_params* best,
+                           double* best_ms);
 
 /* Step budget of one launch (total step attempts over all rays; 0 = none).
    A launch that exceeds it stops taking rays and returns BH_ERR_BUDGET. */

@@ -241,6 +241,25 @@ def test_autotune_keeps_results_and_picks_a_shape(renderer):
         renderer.set_launch(precision=abi.PRECISION_MIXED, **{k: v for k, v in old.items()})
 
 
+def test_autotune_batch_picks_a_shape_in_the_search_space(renderer):
+    cfgs = [kerr_a09_i60(width=40, height=24, precision=abi.PRECISION_MIXED),
+            kerr_a09_i60(width=24, height=40, spin=0.5, precision=abi.PRECISION_MIXED)]
+    before = renderer.render_batch(cfgs)
+    old = renderer.get_launch(abi.PRECISION_MIXED)
+    try:
+        best, ms = renderer.autotune_batch(cfgs)
+        assert ms > 0
+        assert best["block_size"] in (64, 128, 256, 512) and best["rays_per_thread"] in (1, 2, 4, 8)
+        assert best["refill"] in (8, 16, 24, 32) and best["reg_variant"] in (1, 2)
+        assert renderer.get_launch(abi.PRECISION_MIXED) == best
+        for a, b in zip(before, renderer.render_batch(cfgs)):
+            lit = a[..., 1] > 0
+            rel = np.abs(a[..., 1][lit] - b[..., 1][lit]) / a[..., 1][lit]
+            assert q(rel, 0.99) <= 1e-2      # the two register caps are two compilations
+    finally:
+        renderer.set_launch(precision=abi.PRECISION_MIXED, **{k: v for k, v in old.items()})
+
+
 def test_stats_accumulate_like_reference(renderer):
     cfg = kerr_a09_i60(width=32, height=32)
     st = RenderStats()
