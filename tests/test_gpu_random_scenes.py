@@ -1,0 +1,61 @@
+"""Seeded random scenes: the FP64 GPU path against the CPU oracle (which is
+pinned bit for bit to the reference) and the mixed path against the FP64 GPU
+path, over spins, inclinations, camera distances, fields of view, disc
+extents, senses, samples per pixel, sky and stop rules chosen at random.
+Each scene is a small window, so the oracle finishes in seconds."""
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from parity import compare, q, summary  # noqa: E402
+
+from blackhole_b200 import abi  # noqa: E402
+from blackhole_b200.config import M_SUN, Camera, RenderConfig  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(seed):
+    rng = np.random.default_rng(seed)
+    r_cam = float(rng.uniform(40.0, 2000.0))
+    half = float(rng.uniform(6.0, 40.0))
+    cfg = RenderConfig(
+        M_kg=float(10 ** rng.uniform(0.5, 9.5)) * M_SUN,
+        spin=float(rng.choice([0.0, rng.uniform(-0.99, 0.99), 0.998])),
+        cam=Camera(r=r_cam, theta=math.radians(float(rng.uniform(3.0, 177.0))),
+                   phi=float(rng.uniform(0, 2 * math.pi)), fov=2.0 * math.atan(half / r_cam),
+                   yaw=float(rng.normal(0, 0.002)), pitch=float(rng.normal(0, 0.002)),
+                   roll=float(rng.uniform(-0.5, 0.5))),
+        width=32, height=24, sqrt_spp=int(rng.integers(1, 3)),
+        disc_enabled=bool(rng.random() < 0.85), disc_r_out=float(rng.uniform(8.0, 60.0)),
+        eddington=float(10 ** rng.uniform(-4, 0)), disc_sense=int(rng.choice([1, -1])),
+        star_count=int(rng.integers(0, 50000)), seed=int(rng.integers(0, 2**63)),
+        rtol=1e-8, atol=1e-10, r_escape=1.1 * r_cam, quiet=True,
+        sky_mode=int(rng.integers(0, 2)), stop_mode=int(rng.integers(0, 2)), stop_epsilon=1e-6,
+    )
+    return cfg
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_scene_fp64_matches_oracle_and_mixed_meets_target(renderer, orc, seed):
+    cfg = _scene(seed)
+    cfg.precision = abi.PRECISION_FP64
+    chk, _ = orc.trace_rays(cfg)
+    g64 = renderer.trace_rays(cfg)
+    s = compare(g64, chk)
+    msg = f"seed {seed}: {summary(s)}"
+    assert s["class_agree"] >= 0.97, msg
+    for k in ("g_rel", "dir_rad", "Y_rel"):
+        assert q(s[k], 0.95) <= 1e-6, msg
+    cfg.precision = abi.PRECISION_MIXED
+    gm = renderer.trace_rays(cfg)
+    sm = compare(gm, g64)
+    msg = f"seed {seed} mixed: {summary(sm)}"
+    assert sm["class_agree"] >= 0.95, msg
+    for k, tol in (("g_rel", 1e-3), ("dir_rad", 1e-4)):
+        if len(sm[k]):
+            assert (sm[k] <= tol).mean() >= 0.97, msg
