@@ -175,6 +175,9 @@ class bh_grad4(C.Structure):
         ("rays", C.c_longlong), ("steps", C.c_longlong), ("replayed_steps", C.c_longlong),
         ("disc_rays", C.c_longlong), ("sky_rays", C.c_longlong),
         ("max_checkpoint_interval", C.c_int32), ("reserved", C.c_int32),
+        ("edge_spin", C.c_double), ("edge_inclination", C.c_double),
+        ("edge_candidates", C.c_longlong), ("edge_cells", C.c_longlong), ("edge_steps", C.c_longlong),
+        ("held_spin", C.c_double), ("held_inclination", C.c_double), ("high_order_rays", C.c_longlong),
     ]
 
     def as_dict(self) -> dict:

@@ -7,9 +7,25 @@
 // Loss = sum over pixels of (Y_pixel - target)^2, Y_pixel being the sample
 // mean of the rendered frame (bh_gpu_render's output).
 //
-// adjoint_reduce_kernel: five blocks, each summing one quantity (the loss and
-// the four gradient components) over a fixed thread-to-element assignment and
-// a fixed tree, so the result does not depend on the order rays finished in.
+// edge_candidates_kernel, edge_kernel: the edge pass.  A point-sampled frame
+// has no derivative with respect to r_out, and its derivatives with respect
+// to the spin and the inclination miss the motion of the disc's edges; the
+// derivative of the frame averaged over each sample's cell has both.  Each
+// sample's first two equatorial crossings near an edge (adj::edge_mask,
+// against the spread of the neighbouring samples' same crossing) get the
+// edge term of adj::edge_sample with weight 2 (Y_pixel - target).
+//
+// The edge pass covers the edges of the first two equatorial crossings (the
+// direct image of the disc and its first lensed image).  Images of order
+// three and higher are rings so thin that a sample's derivative holds over a
+// small part of its cell, and their edges are not in the edge pass, so their
+// per-ray spin and inclination terms are summed apart (the held-out sums)
+// rather than into the frame gradient.
+//
+// adjoint_reduce_kernel: ten blocks, each summing one quantity (the loss,
+// the four per-ray gradient components, the three edge components, the two
+// held-out components) over a fixed thread-to-element assignment and a fixed
+// tree, so the result does not depend on the order rays finished in.
 #include <cuda_runtime.h>
 
 #include "bh_adjoint.cuh"
@@ -28,7 +44,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const AdjointLaunch 
     const int S = L.frame.S;
     const int SS = S * S;
     const int W = L.frame.width, H = L.frame.height;
-    unsigned long long steps = 0, replay = 0, disc = 0, sky = 0, max_int = 0;
+    unsigned long long steps = 0, replay = 0, disc = 0, sky = 0, max_int = 0, n_high = 0;
     for (;;) {
         const long long id = (long long)atomicAdd(&L.counters[0], 1ull);
         if (id >= L.n_rays) break;
@@ -39,8 +55,20 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const AdjointLaunch 
         const long long pix = (long long)py * W + px;
         const double w = 2.0 * (L.pixels[pix].y - (double)L.target[pix]) / (double)SS;
         adj::RayResult res;
-        adj::adjoint_ray(L.frame, L.X, L.sky, id, w, ck, slots, false, &res);
+        adj::Crossings xr;
+        xr.n = 0;
+        xr.count = 0;
+        xr.r[0] = xr.r[1] = 0.0;
+        xr.step[0] = xr.step[1] = 0;
+        adj::adjoint_ray(L.frame, L.X, L.sky, id, w, ck, slots, false, &res, &xr);
         const long long o = pix * SS + k;
+        L.xing_r[2 * o] = xr.r[0];
+        L.xing_r[2 * o + 1] = xr.r[1];
+        L.xing_step[2 * o] = xr.step[0];
+        L.xing_step[2 * o + 1] = xr.step[1];
+        const bool high = xr.count >= 3 && (res.what == BH_HIT_DISC || res.what == BH_HIT_SKY);
+        L.high_order[o] = high ? 1 : 0;
+        n_high += high ? 1ull : 0ull;
         #pragma unroll
         for (int q = 0; q < 4; ++q) L.ray_grad[o * 4 + q] = res.grad[q];
         if (L.ray_Y) L.ray_Y[o] = res.Y;
@@ -55,10 +83,84 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const AdjointLaunch 
     atomicAdd(&L.counters[3], disc);
     atomicAdd(&L.counters[4], sky);
     atomicMax(&L.counters[5], max_int);
+    atomicAdd(&L.counters[10], n_high);
+}
+
+// Candidate selection: one thread per sample; each of its first two
+// equatorial crossings is compared with the same crossing of its four
+// neighbours in the W S x H S sample grid (adj::edge_mask).
+__global__ void __launch_bounds__(256) edge_candidates_kernel(const AdjointLaunch L) {
+    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= L.n_rays) return;
+    const int S = L.frame.S;
+    const int SS = S * S;
+    const long long pix = o / SS;
+    const int k = (int)(o - pix * SS);
+    const int W = L.frame.width, H = L.frame.height;
+    const int gx = (int)(pix % W) * S + k % S;
+    const int gy = (int)(pix / W) * S + k / S;
+    const int GW = W * S, GH = H * S;
+    for (int j = 0; j < 2; ++j) {
+        if (L.xing_step[2 * o + j] == 0) break;
+        const double rc = L.xing_r[2 * o + j];
+        double dmax = 0.0;
+        #pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int nx = gx + (n == 0) - (n == 1);
+            const int ny = gy + (n == 2) - (n == 3);
+            if (nx < 0 || nx >= GW || ny < 0 || ny >= GH) continue;
+            const long long on = ((long long)(ny / S) * W + nx / S) * SS + (ny % S) * S + nx % S;
+            if (L.xing_step[2 * on + j] == 0) continue;
+            const double d = fabs(rc - L.xing_r[2 * on + j]);
+            if (d > dmax) dmax = d;
+        }
+        const int m = adj::edge_mask(L.frame, rc, dmax);
+        if (m) {
+            const unsigned long long at = atomicAdd(&L.counters[6], 1ull);
+            L.cand[at] = ((unsigned long long)(2 * o + j) << 2) | (unsigned long long)m;
+        }
+    }
+}
+
+// The edge term of each candidate; candidates handed out by an atomic
+// counter, each thread with its own checkpoint slots, results written per
+// crossing slot so the sums do not depend on the order.
+__global__ void __launch_bounds__(kAdjBlock) edge_kernel(const AdjointLaunch L) {
+    const long long thread = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int slots = L.X.checkpoint_slots;
+    double* ck = L.ckpt + thread * slots * 8;
+    const unsigned long long n_cand = L.counters[6];
+    const int S = L.frame.S;
+    const int SS = S * S;
+    const int W = L.frame.width;
+    unsigned long long steps = 0, cells = 0;
+    for (;;) {
+        const unsigned long long i = atomicAdd(&L.counters[7], 1ull);
+        if (i >= n_cand) break;
+        const unsigned long long c = L.cand[i];
+        const long long slot = (long long)(c >> 2);
+        const int edges = (int)(c & 3ull);
+        const long long o = slot >> 1;
+        const long long pix = o / SS;
+        const int k = (int)(o - pix * SS);
+        const int px = (int)(pix % W), py = (int)(pix / W);
+        const double w = 2.0 * (L.pixels[pix].y - (double)L.target[pix]);
+        double out[3];
+        int n_cells = 0;
+        steps += (unsigned long long)adj::edge_sample(L.frame, L.X, L.sky, px, py, k, L.xing_step[slot], edges, w,
+                                                      ck, slots, out, &n_cells);
+        cells += (unsigned long long)n_cells;
+        L.edge_out[3 * slot] = out[0];
+        L.edge_out[3 * slot + 1] = out[1];
+        L.edge_out[3 * slot + 2] = out[2];
+    }
+    atomicAdd(&L.counters[8], steps);
+    atomicAdd(&L.counters[9], cells);
 }
 
 __global__ void __launch_bounds__(kReduceThreads)
-adjoint_reduce_kernel(const double* __restrict__ grad, long long n_rays, const bh_xyz* __restrict__ pixels,
+adjoint_reduce_kernel(const double* __restrict__ grad, const double* __restrict__ edge,
+                      const unsigned char* __restrict__ high, long long n_rays, const bh_xyz* __restrict__ pixels,
                       const float* __restrict__ target, long long n_pix, double* out) {
     __shared__ double part[kReduceThreads];
     const int b = blockIdx.x;
@@ -68,8 +170,16 @@ adjoint_reduce_kernel(const double* __restrict__ grad, long long n_rays, const b
             const double d = pixels[p].y - (double)target[p];
             acc += d * d;
         }
-    } else {
+    } else if (b <= 2) {           // spin, inclination: images of order one and two
+        for (long long i = threadIdx.x; i < n_rays; i += kReduceThreads)
+            if (!high[i]) acc += grad[i * 4 + (b - 1)];
+    } else if (b <= 4) {           // Eddington ratio, r_out: every ray
         for (long long i = threadIdx.x; i < n_rays; i += kReduceThreads) acc += grad[i * 4 + (b - 1)];
+    } else if (b <= 7) {
+        for (long long i = threadIdx.x; i < 2 * n_rays; i += kReduceThreads) acc += edge[i * 3 + (b - 5)];
+    } else {                       // spin, inclination: order three and higher
+        for (long long i = threadIdx.x; i < n_rays; i += kReduceThreads)
+            if (high[i]) acc += grad[i * 4 + (b - 8)];
     }
     part[threadIdx.x] = acc;
     __syncthreads();
@@ -91,12 +201,16 @@ int adjoint_blocks_per_sm(int block_size) {
 
 cudaError_t launch_adjoint(const AdjointLaunch& L, cudaStream_t stream) {
     if (L.block != kAdjBlock) return cudaErrorInvalidValue;
-    if (L.n_rays > 0) adjoint_kernel<<<L.grid, L.block, 0, stream>>>(L);
+    if (L.n_rays > 0) {
+        adjoint_kernel<<<L.grid, L.block, 0, stream>>>(L);
+        edge_candidates_kernel<<<(unsigned)((L.n_rays + 255) / 256), 256, 0, stream>>>(L);
+        edge_kernel<<<L.grid, L.block, 0, stream>>>(L);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const long long n_pix = (long long)L.frame.width * L.frame.height;
-    adjoint_reduce_kernel<<<5, kReduceThreads, 0, stream>>>(L.ray_grad, L.n_rays, L.pixels, L.target, n_pix,
-                                                           L.sums);
+    adjoint_reduce_kernel<<<kAdjSums, kReduceThreads, 0, stream>>>(L.ray_grad, L.edge_out, L.high_order,
+                                                                  L.n_rays, L.pixels, L.target, n_pix, L.sums);
     return cudaGetLastError();
 }
 

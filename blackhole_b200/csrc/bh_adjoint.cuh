@@ -25,12 +25,15 @@
 //   4. the adjoint of the initial photon is contracted with the derivatives of
 //      the initial state (camera tetrad and metric at the camera).
 //
-// The disc's outer edge is a step in the image: a ray's luminance does not
-// depend on r_out except when its crossing radius passes r_out, so the
-// derivative of a point-sampled frame with respect to r_out is zero, and the
-// edges of the disc and of the shadow contribute to finite differences of
-// the frame through the pixels that change class (a boundary term this
-// per-ray adjoint does not contain).
+// The disc's edges are steps in the image: a ray's luminance does not depend
+// on r_out except when its crossing radius passes r_out, so the derivative of
+// a point-sampled frame with respect to r_out is zero, and the edges move
+// with the spin and the inclination too.  The edge term (edge_sample below)
+// is the derivative of the frame averaged over each sample's cell: for a
+// crossing near an edge, the luminance jump times the edge's length in the
+// cell times its speed, the image-plane gradient of the crossing radius and
+// its parameter derivatives coming from a reverse sweep seeded with that
+// radius.
 //
 // All arithmetic is binary64.  The functions compile for the host as well, so
 // the same code can be checked against finite differences on a CPU.
@@ -688,23 +691,40 @@ struct RayResult {
 // Initial photon of frame-local ray `local_id` (render.cpp:440-451,
 // scene.h:356-384, geodesic.h:215-231) and its derivatives with respect to
 // the spin and the inclination.
-__host__ __device__ inline void ray_start(const FrameParams& F, const AdjointFrame& X, long long local_id,
-                                          double y[6], double* E, double* Lz, double dy[2][6], double dE[2],
-                                          double dLz[2]) {
+// The image-plane position of sample k of pixel (px, py) (scene.h:356-384
+// with the render path's jitter): su, sv in [-1, 1]; *x_pix, *y_pix in pixels.
+__host__ __device__ inline void sample_position_at(const FrameParams& F, int px, int py, int k, double* su,
+                                                   double* sv, double* x_pix, double* y_pix) {
     const int S = F.S;
-    const long long pixel = local_id / (S * S);
-    const int k = (int)(local_id - pixel * (S * S));
     const int sy = k / S, sx = k - (k / S) * S;
-    int px, py;
-    pixel_xy(F.width, F.height, pixel, &px, &py);
     const uint64_t s0 = F.seed ^ ((uint64_t)py << 32) ^ ((uint64_t)px * 0x9E3779B97F4A7C15ull);
     const uint64_t g = 0x9E3779B97F4A7C15ull;
     const double u1 = u53(mix64(s0 + (uint64_t)(2 * k + 1) * g));
     const double u2 = u53(mix64(s0 + (uint64_t)(2 * k + 2) * g));
     const double jx = xm(xa((double)sx, u1), F.inv_S);
     const double jy = xm(xa((double)sy, u2), F.inv_S);
-    const double su = xs(xd(xm(2.0, xa((double)px, jx)), (double)F.width), 1.0);
-    const double sv = xs(1.0, xd(xm(2.0, xa((double)py, jy)), (double)F.height));
+    *x_pix = xa((double)px, jx);
+    *y_pix = xa((double)py, jy);
+    *su = xs(xd(xm(2.0, *x_pix), (double)F.width), 1.0);
+    *sv = xs(1.0, xd(xm(2.0, *y_pix), (double)F.height));
+}
+
+// The same for frame-local sample `local_id` (work order).
+__host__ __device__ inline void sample_position(const FrameParams& F, long long local_id, double* su, double* sv,
+                                                double* x_pix, double* y_pix) {
+    const int S = F.S;
+    const long long pixel = local_id / (S * S);
+    const int k = (int)(local_id - pixel * (S * S));
+    int px, py;
+    pixel_xy(F.width, F.height, pixel, &px, &py);
+    sample_position_at(F, px, py, k, su, sv, x_pix, y_pix);
+}
+
+// The initial photon at image-plane position (su, sv) and its derivatives
+// with respect to the spin and the inclination.
+__host__ __device__ inline void ray_start_at(const FrameParams& F, const AdjointFrame& X, double su, double sv,
+                                             double y[6], double* E, double* Lz, double dy[2][6], double dE[2],
+                                             double dLz[2]) {
     double x = xm(su, F.tanf);
     double yy = xd(xm(sv, F.tanf), F.aspect);
     const double z = 1.0;
@@ -754,18 +774,137 @@ __host__ __device__ inline void ray_start(const FrameParams& F, const AdjointFra
     }
 }
 
+// The initial photon of frame-local sample `local_id`.
+__host__ __device__ inline void ray_start(const FrameParams& F, const AdjointFrame& X, long long local_id,
+                                          double y[6], double* E, double* Lz, double dy[2][6], double dE[2],
+                                          double dLz[2]) {
+    double su, sv, xp, yp;
+    sample_position(F, local_id, &su, &sv, &xp, &yp);
+    ray_start_at(F, X, su, sv, y, E, Lz, dy, dE, dLz);
+}
+
 // Accepted steps of the replay buffer: the reverse pass recomputes a segment
 // in pieces of at most this many steps.
 constexpr int kReplay = 16;
 
-// The forward pass, the seed and the reverse pass of one ray.  `ck` holds
-// `slots` checkpoints of 8 doubles.  With w == 0 (or forward_only) only the
-// luminance is computed.
-__host__ __device__ inline void adjoint_ray(const FrameParams& F, const AdjointFrame& X, const SkyData& sky,
-                                            long long local_id, double w, double* ck, int slots,
-                                            bool forward_only, RayResult* out) {
-    double y0[6], E, Lz, dy0[2][6], dE[2], dLz[2];
-    ray_start(F, X, local_id, y0, &E, &Lz, dy0, dE, dLz);
+// Checkpoint store of one ray: `slots` states of 8 doubles (y, h, err_prev)
+// after every `interval` accepted steps; full slots drop every second state
+// and double the interval.
+struct Checkpoints {
+    double* ck;
+    int slots;
+    int interval;
+    int n;
+    __host__ __device__ void push(const Integ& st) {
+        double* p = ck + 8 * n;
+        for (int i = 0; i < 6; ++i) p[i] = st.y[i];
+        p[6] = st.h;
+        p[7] = st.err_prev;
+        ++n;
+    }
+    __host__ __device__ void after_step(const Integ& st) {
+        if (st.steps % interval != 0) return;
+        if (n == slots) {
+            for (int j = 0; j < slots / 2; ++j)
+                for (int i = 0; i < 8; ++i) ck[8 * j + i] = ck[8 * (2 * j) + i];
+            n = slots / 2;
+            interval *= 2;
+        }
+        if (st.steps % interval == 0) push(st);
+    }
+};
+
+// The first two equatorial crossings of a ray: their radii and the accepted
+// steps they lie in (0: none); `count` counts all of them.
+struct Crossings {
+    double r[2];
+    int step[2];
+    int n;
+    int count;
+};
+
+// Integrates from `s` with the render path's events (render.cpp:158-257)
+// until the ray ends, returning its class, or until accepted step `stop_at`
+// has been taken, returning -1 before that step's events are looked at.  The
+// crossing radius of a disc hit goes to *r_hit.  Checkpoints (cp) and the
+// first two equatorial crossings (xr) are recorded when given.
+__host__ __device__ inline int forward_run(const FrameParams& F, const RayC& c, Integ& s, Checkpoints* cp,
+                                           Crossings* xr, int stop_at, double* r_hit) {
+    if (F.max_steps <= 0) return BH_HIT_EXHAUSTED;
+    StepRec rec;
+    for (;;) {
+        if (!advance(F, c, s, &rec)) return BH_HIT_HORIZON;   // no acceptable step (render.cpp:133-136)
+        if (s.steps == stop_at) return -1;
+        const double rn = rec.yn[1];
+        if (rn <= F.r_stop) return BH_HIT_HORIZON;
+        if (F.disc_enabled && rec.c0 * rec.c7 < 0.0) {
+            const DenseC cth = dense_coef(rec.h, rec.y[2], rec.yn[2], rec.kth[0], rec.kth[2], rec.kth[3],
+                                          rec.kth[4], rec.kth[5], rec.kth[6]);
+            const double s_end = dense_crossing(cth, crossing_target(cth.r1, cth.r1 + cth.r2));
+            const DenseC crr = dense_coef(rec.h, rec.y[1], rec.yn[1], rec.kr[0], rec.kr[2], rec.kr[3],
+                                          rec.kr[4], rec.kr[5], rec.kr[6]);
+            const double rc = dense_eval(crr, s_end);
+            if (xr) {
+                if (xr->n < 2) {
+                    xr->r[xr->n] = rc;
+                    xr->step[xr->n++] = s.steps;
+                }
+                ++xr->count;
+            }
+            if (rc >= F.r_in && rc <= F.r_out) {
+                *r_hit = rc;
+                return BH_HIT_DISC;
+            }
+        }
+        if (rn > F.r_escape) return BH_HIT_SKY;
+        if (s.steps >= F.max_steps) return BH_HIT_EXHAUSTED;
+        if (cp) cp->after_step(s);
+    }
+}
+
+// The reverse pass: carries the adjoint yb of the state after accepted step N
+// (and, when rstar_b != 0, the weight of the disc-crossing radius of step N)
+// back to the initial photon, segment by segment from the checkpoints, with
+// the E, L_z and spin adjoints accumulated.  Returns the steps replayed.
+__host__ __device__ inline long long reverse_sweep(const FrameParams& F, const RayC& c, const Checkpoints& cp,
+                                                   int N, double rstar_b, double yb[6], double* Eb, double* Lzb,
+                                                   double* ab) {
+    long long replay = 0;
+    const int interval = cp.interval;
+    double ys_buf[kReplay][6], hs_buf[kReplay];
+    for (int seg = (N - 1) / interval; seg >= 0; --seg) {
+        const int first = seg * interval + 1;               // first step of the segment
+        const int last = (first + interval - 1 < N) ? first + interval - 1 : N;
+        const int len = last - first + 1;
+        const int npiece = (len + kReplay - 1) / kReplay;
+        for (int piece = npiece - 1; piece >= 0; --piece) {
+            Integ r;
+            const double* p = cp.ck + 8 * seg;
+            for (int i = 0; i < 6; ++i) r.y[i] = p[i];
+            r.h = p[6];
+            r.err_prev = p[7];
+            r.have_k1 = 0;
+            r.tries = 0;
+            r.steps = 0;
+            for (int j = 0; j < piece * kReplay; ++j) advance(F, c, r, nullptr);
+            const int m = (len - piece * kReplay < kReplay) ? len - piece * kReplay : kReplay;
+            for (int j = 0; j < m; ++j) {
+                StepRec q;
+                advance(F, c, r, &q);
+                for (int i = 0; i < 6; ++i) ys_buf[j][i] = q.y[i];
+                hs_buf[j] = q.h;
+            }
+            replay += piece * kReplay + m;
+            for (int j = m - 1; j >= 0; --j) {
+                const bool final_step = first + piece * kReplay + j == N;
+                step_vjp(c, ys_buf[j], hs_buf[j], yb, Eb, Lzb, ab, final_step ? rstar_b : 0.0);
+            }
+        }
+    }
+    return replay;
+}
+
+__host__ __device__ inline RayC ray_consts(const FrameParams& F, double E, double Lz) {
     RayC c;
     c.a = F.a;
     c.a2 = F.a2;
@@ -774,75 +913,41 @@ __host__ __device__ inline void adjoint_ray(const FrameParams& F, const AdjointF
     c.rp = F.r_plus;
     c.rm = F.r_minus;
     c.factored = F.factored_delta;
-    out->Y = 0.0;
-    for (int q = 0; q < 4; ++q) out->grad[q] = 0.0;
-    out->replay = 0;
+    return c;
+}
 
-    Integ s;
+__host__ __device__ inline void integ_start(const FrameParams& F, const double y0[6], Integ& s) {
     for (int i = 0; i < 6; ++i) s.y[i] = y0[i];
     s.h = F.h0;
     s.err_prev = 1e-4;
     s.have_k1 = 0;
     s.tries = 0;
     s.steps = 0;
-    int interval = X.checkpoint_interval;
-    int nck = 0;
-    auto push = [&](const Integ& st) {
-        double* p = ck + 8 * nck;
-        for (int i = 0; i < 6; ++i) p[i] = st.y[i];
-        p[6] = st.h;
-        p[7] = st.err_prev;
-        ++nck;
-    };
-    push(s);
-    int what = BH_HIT_EXHAUSTED;
+}
+
+// The forward pass, the seed and the reverse pass of one ray.  `ck` holds
+// `slots` checkpoints of 8 doubles.  With w == 0 (or forward_only) only the
+// luminance is computed.  xr (may be null) receives the ray's first two
+// equatorial crossings.
+__host__ __device__ inline void adjoint_ray(const FrameParams& F, const AdjointFrame& X, const SkyData& sky,
+                                            long long local_id, double w, double* ck, int slots,
+                                            bool forward_only, RayResult* out, Crossings* xr = nullptr) {
+    double y0[6], E, Lz, dy0[2][6], dE[2], dLz[2];
+    ray_start(F, X, local_id, y0, &E, &Lz, dy0, dE, dLz);
+    const RayC c = ray_consts(F, E, Lz);
+    out->Y = 0.0;
+    for (int q = 0; q < 4; ++q) out->grad[q] = 0.0;
+    out->replay = 0;
+
+    Integ s;
+    integ_start(F, y0, s);
+    Checkpoints cp{ck, slots, X.checkpoint_interval, 0};
+    cp.push(s);
     double r_hit = 0.0;
-    StepRec rec;
-    if (F.max_steps > 0) {
-        for (;;) {
-            if (!advance(F, c, s, &rec)) {
-                what = BH_HIT_HORIZON;   // no acceptable step (render.cpp:133-136)
-                break;
-            }
-            const double rn = rec.yn[1];
-            int ev = -1;
-            if (rn <= F.r_stop) {
-                ev = BH_HIT_HORIZON;
-            } else if (F.disc_enabled && rec.c0 * rec.c7 < 0.0) {
-                const DenseC cth = dense_coef(rec.h, rec.y[2], rec.yn[2], rec.kth[0], rec.kth[2], rec.kth[3],
-                                              rec.kth[4], rec.kth[5], rec.kth[6]);
-                const double s_end = dense_crossing(cth, crossing_target(cth.r1, cth.r1 + cth.r2));
-                const DenseC crr = dense_coef(rec.h, rec.y[1], rec.yn[1], rec.kr[0], rec.kr[2], rec.kr[3],
-                                              rec.kr[4], rec.kr[5], rec.kr[6]);
-                const double rc = dense_eval(crr, s_end);
-                if (rc >= F.r_in && rc <= F.r_out) {
-                    ev = BH_HIT_DISC;
-                    r_hit = rc;
-                }
-            }
-            if (ev < 0 && rn > F.r_escape) ev = BH_HIT_SKY;
-            if (ev >= 0) {
-                what = ev;
-                break;
-            }
-            if (s.steps >= F.max_steps) {
-                what = BH_HIT_EXHAUSTED;
-                break;
-            }
-            if (s.steps % interval == 0) {
-                if (nck == slots) {
-                    for (int j = 0; j < slots / 2; ++j)
-                        for (int i = 0; i < 8; ++i) ck[8 * j + i] = ck[8 * (2 * j) + i];
-                    nck = slots / 2;
-                    interval *= 2;
-                }
-                if (s.steps % interval == 0) push(s);
-            }
-        }
-    }
+    const int what = forward_run(F, c, s, &cp, xr, -1, &r_hit);
     out->what = what;
     out->steps = s.steps;
-    out->interval = interval;
+    out->interval = cp.interval;
 
     // ---- seed --------------------------------------------------------------------
     double yb[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -875,45 +980,232 @@ __host__ __device__ inline void adjoint_ray(const FrameParams& F, const AdjointF
         yb[3] == 0.0 && yb[4] == 0.0 && yb[5] == 0.0)
         return;
 
-    // ---- reverse -------------------------------------------------------------------
-    const int N = s.steps;
-    double ys_buf[kReplay][6], hs_buf[kReplay];
-    for (int seg = (N - 1) / interval; seg >= 0; --seg) {
-        const int first = seg * interval + 1;               // first step of the segment
-        const int last = (first + interval - 1 < N) ? first + interval - 1 : N;
-        const int len = last - first + 1;
-        const int npiece = (len + kReplay - 1) / kReplay;
-        for (int piece = npiece - 1; piece >= 0; --piece) {
-            Integ r;
-            const double* p = ck + 8 * seg;
-            for (int i = 0; i < 6; ++i) r.y[i] = p[i];
-            r.h = p[6];
-            r.err_prev = p[7];
-            r.have_k1 = 0;
-            r.tries = 0;
-            r.steps = 0;
-            for (int j = 0; j < piece * kReplay; ++j) advance(F, c, r, nullptr);
-            const int m = (len - piece * kReplay < kReplay) ? len - piece * kReplay : kReplay;
-            for (int j = 0; j < m; ++j) {
-                StepRec q;
-                advance(F, c, r, &q);
-                for (int i = 0; i < 6; ++i) ys_buf[j][i] = q.y[i];
-                hs_buf[j] = q.h;
-            }
-            out->replay += piece * kReplay + m;
-            for (int j = m - 1; j >= 0; --j) {
-                const bool final_disc = (what == BH_HIT_DISC) && (first + piece * kReplay + j == N);
-                step_vjp(c, ys_buf[j], hs_buf[j], yb, &Eb, &Lzb, &ab, final_disc ? rstar_b : 0.0);
-            }
-        }
-    }
-    // ---- the initial photon -------------------------------------------------------------
+    // ---- reverse and the initial photon ------------------------------------------------
+    out->replay = reverse_sweep(F, c, cp, s.steps, what == BH_HIT_DISC ? rstar_b : 0.0, yb, &Eb, &Lzb, &ab);
     for (int q = 0; q < 2; ++q) {
         double gq = Eb * dE[q] + Lzb * dLz[q];
         for (int i = 0; i < 6; ++i) gq += yb[i] * dy0[q][i];
         out->grad[q] += gq;
     }
     out->grad[kParSpin] += ab;
+}
+
+// ---- the edge term ---------------------------------------------------------------------
+//
+// A point-sampled frame changes with r_out only where a sample's equatorial
+// crossing radius r_c passes the edge, so the discrete adjoint above has no
+// r_out term.  The derivative of the frame averaged over each sample's cell
+// of the pixel has one: with r_c linear in the image plane across the cell,
+//   d(pixel)/d(r_out)  =  (Y_in - Y_out) L / |grad r_c|,
+// L the length of the line r_c = r_out inside the cell (pixel units), Y_in
+// the disc's luminance at r_out along the ray (the same E, L_z), Y_out what
+// the ray sees when this crossing misses the disc (its continuation traced
+// on).  The same edge moves with any parameter q that moves r_c, which adds
+//   -(Y_in - Y_out) (d r_c/d q) L / |grad r_c|
+// to d(pixel)/dq.  grad r_c and d r_c/dq come from a reverse sweep seeded
+// with the crossing radius alone.
+
+// d(initial p_r, p_th, E, L_z)/d(su, sv): the image-plane coordinates of
+// scene.h:356-384 (su = 2 (x + jx)/W - 1, sv = 1 - 2 (y + jy)/H).
+__host__ __device__ inline void ray_start_pixel_tangents(const FrameParams& F, double su0, double sv0,
+                                                         double dpr[2], double dpth[2], double dE[2],
+                                                         double dLz[2]) {
+    using D2 = Dual<2>;
+    const D2 su = D2::var(su0, 0), sv = D2::var(sv0, 1);
+    D2 x = su * F.tanf;
+    D2 yy = sv * F.tanf / F.aspect;
+    if (F.has_roll) {
+        const D2 xr = F.cr * x - F.sr * yy;
+        const D2 yr = F.sr * x + F.cr * yy;
+        x = xr;
+        yy = yr;
+    }
+    const D2 y2 = F.cp * yy - F.sp;
+    const D2 z2 = F.sp * yy + F.cp;
+    const D2 x2 = F.cy * x + F.sy * z2;
+    const D2 z3 = -F.sy * x + F.cy * z2;
+    const D2 v0 = -z3, v1 = -y2, v2 = x2;
+    const D2 n = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    const D2 d0 = v0 / n, d1 = v1 / n, d2 = v2 / n;
+    for (int k = 0; k < 2; ++k) {
+        const double p1 = d0.d[k] * F.tet11, p2 = d1.d[k] * F.tet22, p3 = d2.d[k] * F.tet33;
+        dpr[k] = F.ml_rr * p1;
+        dpth[k] = F.ml_thth * p2;
+        dE[k] = -(F.ml_tp * p3);
+        dLz[k] = F.ml_pp * p3;
+    }
+}
+
+// Length of the line g . (x - c) = rhs inside the rectangle [x0, x1] x [y0, y1].
+__host__ __device__ inline double line_in_cell(double gx, double gy, double cx, double cy, double rhs, double x0,
+                                               double x1, double y0, double y1) {
+    double px[4], py[4];
+    int n = 0;
+    if (gy != 0.0) {
+        for (int e = 0; e < 2; ++e) {
+            const double x = e ? x1 : x0;
+            const double y = cy + (rhs - gx * (x - cx)) / gy;
+            if (y >= y0 && y <= y1) { px[n] = x; py[n] = y; ++n; }
+        }
+    }
+    if (gx != 0.0) {
+        for (int e = 0; e < 2; ++e) {
+            const double y = e ? y1 : y0;
+            const double x = cx + (rhs - gy * (y - cy)) / gx;
+            if (x >= x0 && x <= x1) { px[n] = x; py[n] = y; ++n; }
+        }
+    }
+    double best = 0.0;
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+            const double dx = px[i] - px[j], dy = py[i] - py[j];
+            const double l = sqrt(dx * dx + dy * dy);
+            if (l > best) best = l;
+        }
+    return best;
+}
+
+// Edges of the disc an equatorial crossing can be near.
+enum { kEdgeOuter = 1, kEdgeInner = 2 };
+
+// The edge term of the equatorial crossing in accepted step `step` of sample k
+// of pixel (px, py), for the disc edges in `edges` (kEdgeOuter: r_out;
+// kEdgeInner: r_in, the ISCO) and pixel weight w = dLoss/d(pixel).  With
+// phi = r_out - r_c (outer) or r_c - r_in (inner), positive on the disc side,
+//   d(pixel)/dq = (Y_disc - Y_beyond) (d phi/d q) L / |grad r_c|.
+// out[0..2] receive the contributions to dLoss/d(r_out), d(spin),
+// d(inclination); *cells the number of edges that cross the sample's cell.
+// diag (may be null) receives r_c, |grad r_c| (per pixel), d r_c/d(spin,
+// inclination), d r_c/d(su, sv), and per edge (outer, inner) L and
+// Y_disc - Y_beyond.  Returns the accepted steps integrated (forward,
+// continuation and replay).
+__host__ __device__ inline long long edge_sample(const FrameParams& F, const AdjointFrame& X, const SkyData& sky,
+                                                 int px, int py, int k, int step, int edges, double w, double* ck,
+                                                 int slots, double out[3], int* cells, double* diag = nullptr) {
+    out[0] = out[1] = out[2] = 0.0;
+    *cells = 0;
+    double su, sv, xp, yp;
+    sample_position_at(F, px, py, k, &su, &sv, &xp, &yp);
+    double y0[6], E, Lz, dy0[2][6], dE[2], dLz[2];
+    ray_start_at(F, X, su, sv, y0, &E, &Lz, dy0, dE, dLz);
+    const RayC c = ray_consts(F, E, Lz);
+    Integ s;
+    integ_start(F, y0, s);
+    Checkpoints cp{ck, slots, X.checkpoint_interval, 0};
+    cp.push(s);
+    double r_hit = 0.0;
+    if (forward_run(F, c, s, &cp, nullptr, step, &r_hit) != -1) return s.steps;
+
+    // What the ray meets when the crossing of that step misses the disc: its
+    // continuation traced on from there.
+    Integ t = s;
+    const int what = forward_run(F, c, t, nullptr, nullptr, -1, &r_hit);
+    long long work = t.steps;
+    double Y_beyond = 0.0;
+    if (what == BH_HIT_DISC) {
+        Y_beyond = disc_luminance(F, X, sky.table, r_hit, E, Lz).v;
+    } else if (what == BH_HIT_SKY) {
+        D8 v[3];
+        if (escape_direction(t.y, E, Lz, F.a, v)) {
+            const double d[3] = {v[0].v, v[1].v, v[2].v};
+            double gY[3];
+            Y_beyond = sky_luminance(sky, F, d, gY);
+        }
+    }
+    // the disc's side of each edge: its luminance at r_out along this ray; the
+    // Novikov-Thorne flux vanishes at r_in
+    const double dY[2] = {(edges & kEdgeOuter) ? disc_luminance(F, X, sky.table, F.r_out, E, Lz).v - Y_beyond : 0.0,
+                          (edges & kEdgeInner) ? -Y_beyond : 0.0};
+    if (dY[0] == 0.0 && dY[1] == 0.0 && !diag) return work;
+
+    // the crossing radius of that step, as the forward pass found it
+    double rc;
+    {
+        const int seg = (step - 1) / cp.interval;
+        const double* p = cp.ck + 8 * seg;
+        Integ r;
+        for (int i = 0; i < 6; ++i) r.y[i] = p[i];
+        r.h = p[6];
+        r.err_prev = p[7];
+        r.have_k1 = 0;
+        r.tries = 0;
+        r.steps = seg * cp.interval;
+        StepRec q;
+        while (r.steps < step) advance(F, c, r, &q);
+        work += step - seg * cp.interval;
+        if (!(q.c0 * q.c7 < 0.0)) return work;   // not a crossing step: nothing to differentiate
+        const DenseC cth = dense_coef(q.h, q.y[2], q.yn[2], q.kth[0], q.kth[2], q.kth[3], q.kth[4], q.kth[5],
+                                      q.kth[6]);
+        const double s_end = dense_crossing(cth, crossing_target(cth.r1, cth.r1 + cth.r2));
+        const DenseC crr = dense_coef(q.h, q.y[1], q.yn[1], q.kr[0], q.kr[2], q.kr[3], q.kr[4], q.kr[5],
+                                      q.kr[6]);
+        rc = dense_eval(crr, s_end);
+    }
+    // d r_c / d(initial state, E, L_z, spin) by a reverse sweep seeded with r_c
+    double yb[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double Eb = 0.0, Lzb = 0.0, ab = 0.0;
+    work += reverse_sweep(F, c, cp, step, 1.0, yb, &Eb, &Lzb, &ab);
+
+    double dpr[2], dpth[2], dEp[2], dLzp[2];
+    ray_start_pixel_tangents(F, su, sv, dpr, dpth, dEp, dLzp);
+    double drc[2];
+    for (int j = 0; j < 2; ++j) drc[j] = yb[4] * dpr[j] + yb[5] * dpth[j] + Eb * dEp[j] + Lzb * dLzp[j];
+    // grad r_c in pixel units: su = 2 x / W - 1, sv = 1 - 2 y / H
+    const double gx = drc[0] * (2.0 / F.width), gy = drc[1] * (-2.0 / F.height);
+    const double gn = sqrt(gx * gx + gy * gy);
+    double drq[2];
+    for (int q = 0; q < 2; ++q) {
+        drq[q] = Eb * dE[q] + Lzb * dLz[q];
+        for (int i = 0; i < 6; ++i) drq[q] += yb[i] * dy0[q][i];
+    }
+    drq[kParSpin] += ab;
+    // the sample's cell in pixel units
+    const int S = F.S;
+    const int sy = k / S, sx = k - (k / S) * S;
+    const double x0 = px + sx * F.inv_S, x1 = px + (sx + 1) * F.inv_S;
+    const double y0c = py + sy * F.inv_S, y1 = py + (sy + 1) * F.inv_S;
+    double L[2] = {0.0, 0.0};
+    for (int e = 0; e < 2; ++e) {
+        if (!(edges & (e == 0 ? kEdgeOuter : kEdgeInner)) || !(gn > 0.0)) continue;
+        const double r_edge = (e == 0) ? F.r_out : F.r_in;
+        L[e] = line_in_cell(gx, gy, xp, yp, r_edge - rc, x0, x1, y0c, y1);
+        if (!(L[e] > 0.0) || dY[e] == 0.0) continue;
+        ++*cells;
+        const double swept = w * dY[e] * L[e] / gn;
+        if (e == 0) {
+            out[0] += swept;
+            out[1] -= swept * drq[kParSpin];
+            out[2] -= swept * drq[kParIncl];
+        } else {
+            out[1] += swept * (drq[kParSpin] - 2.0 * F.x0 * X.d_x0);
+            out[2] += swept * drq[kParIncl];
+        }
+    }
+    if (diag) {
+        diag[0] = rc;
+        diag[1] = gn;
+        diag[2] = drq[0];
+        diag[3] = drq[1];
+        diag[4] = drc[0];
+        diag[5] = drc[1];
+        diag[6] = L[0];
+        diag[7] = dY[0];
+        diag[8] = L[1];
+        diag[9] = dY[1];
+    }
+    return work;
+}
+
+// Whether the crossing at radius rc (sample grid neighbours' same crossing
+// differing by at most dmax; 0 when none has one) is examined for the disc's
+// edges: within twice that spread of an edge, or within a tenth of the edge
+// radius when no neighbour has the crossing.  Returns kEdge* bits.
+__host__ __device__ inline int edge_mask(const FrameParams& F, double rc, double dmax) {
+    int m = 0;
+    auto near = [&](double re) { return dmax > 0.0 ? fabs(rc - re) <= 2.0 * dmax : fabs(rc - re) <= 0.1 * re; };
+    if (rc >= F.r_in && near(F.r_out)) m |= kEdgeOuter;
+    if (rc <= F.r_out && near(F.r_in)) m |= kEdgeInner;
+    return m;
 }
 
 }  // namespace adj

@@ -141,4 +141,109 @@ int bhx_frame_tangents(const bh_render_config* cfg, double out[32]) {
     return BH_OK;
 }
 
+// The first two equatorial crossings of one ray (frame-local id, work
+// order): their radii and accepted steps (0: none); *n_out = how many,
+// *count (may be NULL) = all of the ray's crossings.
+int bhx_crossings(const bh_render_config* cfg, long long local_id, double r[2], int steps[2], int* n_out,
+                  int* count) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    FrameParams F;
+    AdjointFrame X;
+    SkyData sd;
+    const int rc = prepare(cfg, F, X, sd);
+    if (rc != BH_OK) return rc;
+    std::vector<double> ck(static_cast<size_t>(X.checkpoint_slots) * 8);
+    adj::RayResult res;
+    adj::Crossings xr;
+    xr.n = 0;
+    xr.count = 0;
+    xr.r[0] = xr.r[1] = 0.0;
+    xr.step[0] = xr.step[1] = 0;
+    adj::adjoint_ray(F, X, sd, local_id, 0.0, ck.data(), X.checkpoint_slots, true, &res, &xr);
+    for (int k = 0; k < 2; ++k) {
+        r[k] = xr.r[k];
+        steps[k] = xr.step[k];
+    }
+    *n_out = xr.n;
+    if (count) *count = xr.count;
+    return BH_OK;
+}
+
+// The edge term (edge_sample) of the crossing in accepted step `step` of
+// sample k of pixel (px, py) for the edges `edges` (1 outer, 2 inner, 3 both):
+// out = contributions to dLoss/d(r_out, spin, inclination) for pixel weight
+// w; diag = (r_c, |grad r_c|, d r_c/d spin, d r_c/d incl, d r_c/d su,
+// d r_c/d sv, L and dY of the outer edge, L and dY of the inner edge, cells
+// crossed, steps integrated).
+int bhx_edge(const bh_render_config* cfg, int px, int py, int k, int step, int edges, double w, double out[3],
+             double diag[12]) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    FrameParams F;
+    AdjointFrame X;
+    SkyData sd;
+    const int rc = prepare(cfg, F, X, sd);
+    if (rc != BH_OK) return rc;
+    std::vector<double> ck(static_cast<size_t>(X.checkpoint_slots) * 8);
+    for (int i = 0; i < 12; ++i) diag[i] = 0.0;
+    int cells = 0;
+    diag[11] = static_cast<double>(
+        adj::edge_sample(F, X, sd, px, py, k, step, edges, w, ck.data(), X.checkpoint_slots, out, &cells, diag));
+    diag[10] = cells;
+    return BH_OK;
+}
+
+// edge_mask: which edges the crossing at rc is examined for, given the
+// spread dmax of its neighbours' same crossing.
+int bhx_edge_mask(const bh_render_config* cfg, double rc, double dmax, int* mask) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    FrameParams F;
+    AdjointFrame X;
+    SkyData sd;
+    const int rc2 = prepare(cfg, F, X, sd);
+    if (rc2 != BH_OK) return rc2;
+    *mask = adj::edge_mask(F, rc, dmax);
+    return BH_OK;
+}
+
+// The image-plane position (su, sv, x, y in pixels) of sample k of pixel (px, py).
+int bhx_sample_position(const bh_render_config* cfg, int px, int py, int k, double out[4]) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    FrameParams F;
+    AdjointFrame X;
+    SkyData sd;
+    const int rc = prepare(cfg, F, X, sd);
+    if (rc != BH_OK) return rc;
+    adj::sample_position_at(F, px, py, k, &out[0], &out[1], &out[2], &out[3]);
+    return BH_OK;
+}
+
+// The equatorial-crossing radius at accepted step `step` of the ray through
+// image-plane position (su, sv), or NaN when the ray ends before that step.
+int bhx_crossing_radius(const bh_render_config* cfg, double su, double sv, int step, double* r_c) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    FrameParams F;
+    AdjointFrame X;
+    SkyData sd;
+    const int rc = prepare(cfg, F, X, sd);
+    if (rc != BH_OK) return rc;
+    double y0[6], E, Lz, dy0[2][6], dE[2], dLz[2];
+    adj::ray_start_at(F, X, su, sv, y0, &E, &Lz, dy0, dE, dLz);
+    const adj::RayC c = adj::ray_consts(F, E, Lz);
+    adj::Integ s;
+    adj::integ_start(F, y0, s);
+    double r_hit = 0.0;
+    *r_c = std::nan("");
+    if (step > 1 && adj::forward_run(F, c, s, nullptr, nullptr, step - 1, &r_hit) != -1) return BH_OK;
+    adj::StepRec q;
+    if (!adj::advance(F, c, s, &q)) return BH_OK;
+    if (q.c0 * q.c7 >= 0.0) return BH_OK;
+    const DenseC cth = dense_coef(q.h, q.y[2], q.yn[2], q.kth[0], q.kth[2], q.kth[3], q.kth[4],
+                                            q.kth[5], q.kth[6]);
+    const double s_end = dense_crossing(cth, adj::crossing_target(cth.r1, cth.r1 + cth.r2));
+    const DenseC crr = dense_coef(q.h, q.y[1], q.yn[1], q.kr[0], q.kr[2], q.kr[3], q.kr[4], q.kr[5],
+                                            q.kr[6]);
+    *r_c = dense_eval(crr, s_end);
+    return BH_OK;
+}
+
 }  // extern "C"

@@ -259,9 +259,11 @@ class Renderer:
     def adjoint(self, cfg, target, per_ray: bool = False):
         """Loss sum((Y - target)^2) over the pixels of the binary64 frame of
         `cfg` (Y = CIE Y, W m^-2 sr^-1) and its gradient with respect to
-        (spin, inclination, eddington, r_out), as a dict (bh_grad4's fields).
-        With per_ray: also each ray's gradient contribution, shape
-        (n_rays, 4), and luminance, shape (n_rays,), in trace_rays order."""
+        (spin, inclination, eddington, r_out), as a dict (bh_grad4's fields),
+        the disc-edge term included (edge_* fields: its part).  With per_ray:
+        also each ray's discrete-adjoint contribution (edge term not
+        included), shape (n_rays, 4), and luminance, shape (n_rays,), in
+        trace_rays order."""
         c = _as_c(cfg)
         t = np.ascontiguousarray(target, dtype=np.float32)
         if t.size != c.width * c.height:

@@ -353,11 +353,11 @@ int  bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_trace_reco
 /* Result of the discrete adjoint (bh_gpu_adjoint). */
 typedef struct bh_grad4 {
     double loss;             /* sum over pixels of (Y - target)^2, Y the CIE Y of the frame */
-    double d_spin;           /* dLoss / d(spin)                                   */
-    double d_inclination;    /* dLoss / d(camera polar angle cam.theta), per radian */
+    double d_spin;           /* dLoss / d(spin), edge term included               */
+    double d_inclination;    /* dLoss / d(camera polar angle cam.theta), per radian, edge term included */
     double d_eddington;      /* dLoss / d(eddington)                              */
-    double d_r_out;          /* dLoss / d(disc_r_out): 0 (see bh_gpu_adjoint)      */
-    double kernel_ms;        /* device time of the render, adjoint and reductions */
+    double d_r_out;          /* dLoss / d(disc_r_out): the edge term alone        */
+    double kernel_ms;        /* device time of the render, adjoint, edge pass and reductions */
     long long rays;
     long long steps;         /* accepted steps of the adjoint's forward pass      */
     long long replayed_steps;/* accepted steps recomputed by the reverse pass     */
@@ -365,6 +365,14 @@ typedef struct bh_grad4 {
     long long sky_rays;
     int32_t max_checkpoint_interval;
     int32_t reserved;
+    double edge_spin;        /* the edge term's part of d_spin                    */
+    double edge_inclination; /* the edge term's part of d_inclination             */
+    long long edge_candidates;/* equatorial crossings examined for an edge       */
+    long long edge_cells;    /* edges found crossing a sample's cell              */
+    long long edge_steps;    /* accepted steps integrated by the edge pass        */
+    double held_spin;        /* per-ray spin terms of images of order >= 3, not in d_spin */
+    double held_inclination; /* the same for the inclination                     */
+    long long high_order_rays;/* rays whose event came after a third equatorial crossing */
 } bh_grad4;
 
 /* The luminance loss of `cfg` against `target` (W*H floats, row-major, the
@@ -374,18 +382,31 @@ typedef struct bh_grad4 {
    the gradient is the discrete adjoint of that render: each ray's accepted
    DP5 step sequence is replayed backwards from checkpoints (every 16 accepted
    steps, 64 per ray in flight; the interval doubles for longer rays), with
-   the step sizes and each ray's termination class held fixed.  The
-   luminance of a point-sampled frame changes with r_out only where a
-   sample's disc crossing passes the edge, so d_r_out is 0: the edges of the
-   disc and of the shadow act on finite differences of the frame through the
-   samples that change class, a boundary term the per-ray adjoint does not
-   contain.  Scenes with the Sun, a neutron star, a hot spot or a jet return
+   the step sizes and each ray's termination class held fixed.  To that the
+   edge term is added: the motion of the disc's outer edge (r_out) and inner
+   edge (the ISCO) across the image, which a point-sampled frame shows only
+   as samples changing class.  It is the derivative of the frame averaged
+   over each sample's cell of the pixel: for every sample whose first or
+   second equatorial crossing lies near an edge (within twice the spread of
+   the neighbouring samples' same crossing), (luminance jump across the edge)
+   x (length of the edge in the cell) / |image-plane gradient of the
+   crossing radius|, times the edge's speed, the gradient and the speed
+   coming from a reverse sweep of that crossing radius.  d_r_out is that term
+   alone; edge_spin and edge_inclination are its part of d_spin and
+   d_inclination.  The derivative covers the images of the first two
+   equatorial crossings (the direct image and the first lensed image):
+   images of order three and higher are rings thinner than a sample's cell
+   at ordinary resolutions, whose per-sample derivative holds over a small
+   part of the cell, so their per-ray spin and inclination terms are
+   reported apart (held_spin, held_inclination) and their edges are left
+   out.  Scenes with the Sun, a neutron star, a hot spot or a jet return
    BH_ERR_UNSUPPORTED.  No counterpart in the reference. */
 int  bh_gpu_adjoint(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out);
 
 /* bh_gpu_adjoint plus, when not NULL, each ray's gradient contribution
-   (4 doubles: spin, inclination, eddington, r_out) and its luminance, in
-   bh_gpu_trace_rays order (pixel row-major, then sample). */
+   (4 doubles: spin, inclination, eddington, r_out; the per-ray discrete
+   adjoint, without the edge term) and its luminance, in bh_gpu_trace_rays
+   order (pixel row-major, then sample). */
 int  bh_gpu_adjoint_rays(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out,
                          double* ray_grad, double* ray_Y);
 

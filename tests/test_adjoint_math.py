@@ -5,7 +5,11 @@ libbh_adjoint_check.so is the adjoint kernel's own __host__ __device__ code
 it against central finite differences of its own forward pass: the
 right-hand side's vector-Jacobian product, whole rays (disc hits and star-lit
 sky rays) for the spin, inclination and Eddington ratio, and the checkpoint
-thinning, which must not change a single bit of the gradient.
+thinning, which must not change a single bit of the gradient.  For the edge
+term (the motion of the disc's edges across the image): the gradient of an
+equatorial crossing's radius with respect to the image-plane position, the
+spin and the inclination, against central differences of the crossing
+radius, and the rule that picks the crossings examined for an edge.
 """
 import copy
 import ctypes as C
@@ -29,6 +33,13 @@ def chk():
     lib.bhx_rhs.argtypes = [D, D, D]
     lib.bhx_rhs_vjp.argtypes = [D, D, D, D]
     lib.bhx_ray.argtypes = [C.POINTER(abi.bh_render_config), C.c_longlong, C.c_double, C.c_int, C.c_int, D]
+    P = C.POINTER(abi.bh_render_config)
+    I = C.POINTER(C.c_int)
+    lib.bhx_crossings.argtypes = [P, C.c_longlong, D, I, I, I]
+    lib.bhx_edge.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, D, D]
+    lib.bhx_crossing_radius.argtypes = [P, C.c_double, C.c_double, C.c_int, D]
+    lib.bhx_sample_position.argtypes = [P, C.c_int, C.c_int, C.c_int, D]
+    lib.bhx_edge_mask.argtypes = [P, C.c_double, C.c_double, I]
     return lib
 
 
@@ -175,3 +186,142 @@ def test_unsupported_scenes_are_refused(chk):
     out = _a(np.zeros(9))
     c = cfg.to_c()
     assert chk.bhx_ray(C.byref(c), 0, 1.0, 0, 0, _p(out)) == abi.ERR_UNSUPPORTED
+
+
+# ---- the edge term --------------------------------------------------------------------
+
+
+def _isco(a, sense=1):
+    z1 = 1 + (1 - a * a) ** (1 / 3) * ((1 + a) ** (1 / 3) + (1 - a) ** (1 / 3))
+    z2 = math.sqrt(3 * a * a + z1 * z1)
+    return 3 + z2 - sense * math.sqrt((3 - z1) * (3 + z1 + 2 * z2))
+
+
+def _crossings(lib, cfg):
+    """First two equatorial crossings of every sample, in trace_rays order."""
+    n = cfg.width * cfg.height * cfg.sqrt_spp ** 2
+    order = abi.work_order(cfg.width, cfg.height, cfg.sqrt_spp)
+    R = np.zeros((n, 2))
+    ST = np.zeros((n, 2), dtype=np.int64)
+    c = cfg.to_c()
+    r = (C.c_double * 2)()
+    st = (C.c_int * 2)()
+    m = C.c_int()
+    for rid in range(n):
+        assert lib.bhx_crossings(C.byref(c), rid, r, st, C.byref(m), None) == abi.OK
+        R[order[rid]] = r[:]
+        ST[order[rid]] = st[:]
+    return R, ST
+
+
+def _edge(lib, cfg, px, py, k, step, edges, w=1.0):
+    out, diag = _a(np.zeros(3)), _a(np.zeros(12))
+    c = cfg.to_c()
+    assert lib.bhx_edge(C.byref(c), px, py, k, step, edges, w, _p(out), _p(diag)) == abi.OK
+    return out, diag
+
+
+def _rc(lib, cfg, su, sv, step):
+    c = cfg.to_c()
+    r = C.c_double()
+    assert lib.bhx_crossing_radius(C.byref(c), su, sv, step, C.byref(r)) == abi.OK
+    return r.value
+
+
+@pytest.fixture(scope="module")
+def edge_frame(chk):
+    cfg = workloads.adjoint_512()
+    cfg.width = cfg.height = 48
+    R, ST = _crossings(chk, cfg)
+    return cfg, R, ST
+
+
+def test_crossing_radius_gradient_matches_finite_differences(chk, edge_frame):
+    """d r_c/d(su, sv, spin, inclination) from the reverse sweep of the
+    crossing radius, at crossings next to both edges, against central
+    differences of the crossing radius of the same accepted step."""
+    cfg, R, ST = edge_frame
+    r_in = _isco(cfg.spin)
+    picked = []
+    for edge, re in ((1, cfg.disc_r_out), (2, r_in)):
+        near = np.argwhere((ST > 0) & (np.abs(R - re) < 0.05 * re))
+        assert len(near) >= 3, edge
+        picked += [(edge, int(o), int(j)) for o, j in near[:: max(1, len(near) // 3)][:3]]
+    for edge, o, j in picked:
+        px, py = o % cfg.width, o // cfg.width
+        step = int(ST[o, j])
+        _, diag = _edge(chk, cfg, px, py, 0, step, edge)
+        assert diag[0] == pytest.approx(R[o, j], rel=1e-12)
+        pos = _a(np.zeros(4))
+        c = cfg.to_c()
+        assert chk.bhx_sample_position(C.byref(c), px, py, 0, _p(pos)) == abi.OK
+        su, sv = pos[0], pos[1]
+        h = 1e-6
+        fd = [
+            (_rc(chk, _with(cfg, 0, cfg.spin + h), su, sv, step) - _rc(chk, _with(cfg, 0, cfg.spin - h), su, sv, step)) / (2 * h),
+            (_rc(chk, _with(cfg, 1, cfg.cam.theta + h), su, sv, step)
+             - _rc(chk, _with(cfg, 1, cfg.cam.theta - h), su, sv, step)) / (2 * h),
+            (_rc(chk, cfg, su + h, sv, step) - _rc(chk, cfg, su - h, sv, step)) / (2 * h),
+            (_rc(chk, cfg, su, sv + h, step) - _rc(chk, cfg, su, sv - h, step)) / (2 * h),
+        ]
+        scale = max(abs(x) for x in fd)
+        for got, want in zip(diag[2:6], fd):
+            assert got == pytest.approx(want, rel=1e-4, abs=1e-5 * scale), (edge, o, diag[2:6], fd)
+
+
+def test_edge_term_of_a_cell_is_the_swept_area(chk, edge_frame):
+    """For a crossing whose cell the outer edge crosses: the r_out part is
+    w (Y_disc - Y_beyond) L / |grad r_c|, the spin and inclination parts that
+    times -d r_c/dq, and the edge line r_c = r_out (linearised) meets the
+    cell's boundary at both ends of a segment of length L."""
+    cfg, R, ST = edge_frame
+    near = np.argwhere((ST > 0) & (np.abs(R - cfg.disc_r_out) < 0.5))
+    seen = 0
+    for o, j in near:
+        px, py = int(o) % cfg.width, int(o) // cfg.width
+        out, d = _edge(chk, cfg, px, py, 0, int(ST[o, j]), 1, w=3.0)
+        rc, gn, drq, L, dY = d[0], d[1], d[2:4], d[6], d[7]
+        if L == 0.0 or dY == 0.0:
+            assert not out.any()
+            continue
+        assert 0.0 < L <= math.sqrt(2.0) * (1 + 1e-12)
+        swept = 3.0 * dY * L / gn
+        assert out[0] == pytest.approx(swept, rel=1e-12)
+        assert out[1] == pytest.approx(-swept * drq[0], rel=1e-12)
+        assert out[2] == pytest.approx(-swept * drq[1], rel=1e-12)
+        # the line's distance from the sample is |r_out - r_c| / |grad r_c|,
+        # at most the cell's half diagonal from its centre region
+        assert abs(cfg.disc_r_out - rc) / gn <= math.sqrt(2.0)
+        seen += 1
+    assert seen >= 5
+
+
+def test_candidate_rule_finds_every_cell_an_edge_crosses(chk, edge_frame):
+    """Every crossing whose cell an edge crosses (examined with a band of a
+    quarter of the edge radius) is picked by the neighbour-spread rule."""
+    cfg, R, ST = edge_frame
+    W = cfg.width
+    r_in = _isco(cfg.spin)
+    c = cfg.to_c()
+    m = C.c_int()
+    crossed = picked = 0
+    for o in range(W * W):
+        x, y = o % W, o // W
+        for j in range(2):
+            if ST[o, j] == 0:
+                break
+            rc = R[o, j]
+            dmax = 0.0
+            for nx, ny in ((x + 1, y), (x - 1, y), (x, y + 1), (x, y - 1)):
+                if 0 <= nx < W and 0 <= ny < W and ST[ny * W + nx, j] > 0:
+                    dmax = max(dmax, abs(rc - R[ny * W + nx, j]))
+            assert chk.bhx_edge_mask(C.byref(c), rc, dmax, C.byref(m)) == abi.OK
+            for bit, re, ok in ((1, cfg.disc_r_out, rc >= r_in), (2, r_in, rc <= cfg.disc_r_out)):
+                if not ok or abs(rc - re) > 0.25 * re:
+                    continue
+                _, d = _edge(chk, cfg, x, y, 0, int(ST[o, j]), bit)
+                if d[6 if bit == 1 else 8] > 0.0:
+                    crossed += 1
+                    assert m.value & bit, (o, j, bit, rc, dmax)
+                    picked += 1
+    assert crossed >= 20

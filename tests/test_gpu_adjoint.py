@@ -9,10 +9,16 @@
     point: the discrete adjoint holds each ray's events fixed), and over the
     whole frame for the Eddington ratio, which moves no edge;
   - the loss is the sum of squared luminance differences of the render;
-  - repeated calls give identical bits.
+  - repeated calls give identical bits;
+  - the edge term: d/d r_out (the edge term alone) and the whole spin and
+    inclination gradients (per-ray terms of the images of order one and two
+    plus the edge term) against central differences of a supersampled render
+    (64^2 pixels of 8 x 8 samples, where a finite step moves thousands of
+    samples across the disc's edges).
 """
 import copy
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -57,7 +63,7 @@ def c4(renderer):
 
 
 def test_loss_is_the_sum_of_squared_luminance_differences(renderer, c4):
-    cfg, target, g, _, ray_y = c4
+    cfg, target, g, per_ray, ray_y = c4
     Y = _lum(renderer, cfg)
     loss = float(np.sum((Y - target.astype(np.float64)) ** 2))
     assert g["loss"] == pytest.approx(loss, rel=1e-12)
@@ -70,7 +76,10 @@ def test_loss_is_the_sum_of_squared_luminance_differences(renderer, c4):
     assert close.mean() > 0.9995
     assert g["rays"] == cfg.width * cfg.height
     assert g["disc_rays"] > 0 and g["sky_rays"] > 0
-    assert g["d_r_out"] == 0.0
+    # the r_out derivative is the edge term alone
+    assert math.isfinite(g["d_r_out"]) and g["d_r_out"] != 0.0
+    assert g["edge_cells"] > 0 and g["edge_candidates"] >= g["edge_cells"] // 2
+    assert float(per_ray[:, 3].sum()) == 0.0
 
 
 @pytest.mark.parametrize("k,name", [(0, "d_spin"), (1, "d_inclination"), (2, "d_eddington")])
@@ -96,8 +105,11 @@ def test_gradient_matches_central_differences(renderer, c4, k, name):
     fd = float(np.sum((lp - lm)[stable])) / (2 * h)
     adj = float(np.sum(per_ray[:, k].reshape(lp.shape)[stable]))
     assert adj == pytest.approx(fd, rel=GRAD_TOL), (name, adj, fd, int((~stable).sum()))
-    # the frame total is the sum of the per-ray contributions
-    assert g[name] == pytest.approx(float(per_ray[:, k].sum()), rel=1e-12, abs=1e-300)
+    # the frame total is the sum of the per-ray contributions of images of
+    # order one and two and the edge term; the rest is held out
+    edge = {0: g["edge_spin"], 1: g["edge_inclination"], 2: 0.0}[k]
+    held = {0: g["held_spin"], 1: g["held_inclination"], 2: 0.0}[k]
+    assert g[name] - edge + held == pytest.approx(float(per_ray[:, k].sum()), rel=1e-12, abs=1e-300)
     if k == 2:
         assert ((wp == w0) & (wm == w0)).all()
         fd_all = float(np.sum(lp - lm)) / (2 * h)
@@ -107,7 +119,8 @@ def test_gradient_matches_central_differences(renderer, c4, k, name):
 def test_repeated_calls_are_bitwise_identical(renderer, c4):
     cfg, target, g, per_ray, _ = c4
     g2, per_ray2, _ = renderer.adjoint(cfg, target, per_ray=True)
-    for key in ("loss", "d_spin", "d_inclination", "d_eddington"):
+    for key in ("loss", "d_spin", "d_inclination", "d_eddington", "d_r_out", "edge_spin", "edge_inclination",
+                "edge_cells", "edge_candidates"):
         assert g2[key] == g[key]
     assert np.array_equal(per_ray, per_ray2)
 
@@ -181,3 +194,50 @@ def test_photon_ring_crop_gradient_matches_central_differences(renderer, k, name
     fd = float(np.sum((lp - lm)[stable])) / (2 * h)
     adj = float(np.sum(per_ray[:, k].reshape(lp.shape)[stable]))
     assert adj == pytest.approx(fd, rel=GRAD_TOL), (name, adj, fd, int((~stable).sum()))
+
+
+def _supersampled(n, s, target=False):
+    cfg = workloads.adjoint_512(target=target)
+    cfg.width = cfg.height = n
+    cfg.sqrt_spp = s
+    return cfg
+
+
+@pytest.fixture(scope="module")
+def supersampled(renderer):
+    cfg = _supersampled(64, 8)
+    T = _lum(renderer, _supersampled(64, 8, target=True)).astype(np.float32)
+    return cfg, T, renderer.adjoint(cfg, T)
+
+
+def _fd(renderer, cfg, T, k, h):
+    t = T.astype(np.float64)
+    v = _params(cfg)[k]
+    lp = float(np.sum((_lum(renderer, _with(cfg, k, v + h)) - t) ** 2))
+    lm = float(np.sum((_lum(renderer, _with(cfg, k, v - h)) - t) ** 2))
+    return (lp - lm) / (2 * h)
+
+
+def test_r_out_edge_term_matches_supersampled_differences(renderer, supersampled):
+    """d loss / d r_out of a 64^2 frame of 8 x 8 samples per pixel (the
+    edge term: the outer edge's motion across the image) against central
+    differences with a step of 0.25 M, which moves every sample whose
+    crossing lies within 0.25 M of r_out across the edge; 2 % tolerance."""
+    cfg, T, g = supersampled
+    fd = _fd(renderer, cfg, T, 3, 0.25)
+    assert g["d_r_out"] == pytest.approx(fd, rel=0.02), (g["d_r_out"], fd, g["edge_cells"])
+
+
+@pytest.mark.parametrize("k,name", [(0, "d_spin"), (1, "d_inclination")])
+def test_whole_gradient_matches_supersampled_differences(renderer, supersampled, k, name):
+    """The spin and inclination gradients of the same frame (the per-ray
+    terms of images of order one and two and the edge term of both disc
+    edges) against central differences with a step of 0.01; 5 % tolerance.
+    Without the edge term the inclination gradient has the wrong sign here:
+    the disc's outer edge sweeping across the image dominates it."""
+    cfg, T, g = supersampled
+    fd = _fd(renderer, cfg, T, k, 1e-2)
+    assert g[name] == pytest.approx(fd, rel=0.05), (name, g[name], fd)
+    if k == 1:
+        interior = g[name] - g["edge_inclination"]
+        assert np.sign(interior) != np.sign(fd)
