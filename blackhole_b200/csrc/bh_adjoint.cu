@@ -1,19 +1,21 @@
 // bh_adjoint.cu - The discrete-adjoint kernel and its reductions (sm_100a).
 //
-// adjoint_kernel: one thread per ray at a time, rays handed out by a global
+// adjoint_kernel: one thread per job at a time, jobs handed out by a global
 // atomic counter; each thread owns `checkpoint_slots` checkpoint states in
-// global memory for the ray it is working on (bh_adjoint.cuh has the per-ray
-// algorithm).  The ray's loss weight is 2 (Y_pixel - target) / S^2 for
+// global memory for the job it is working on (bh_adjoint.cuh has the per-ray
+// algorithm).  A ray's loss weight is 2 (Y_pixel - target) / S^2 for
 // Loss = sum over pixels of (Y_pixel - target)^2, Y_pixel being the sample
 // mean of the rendered frame (bh_gpu_render's output).
 //
-// edge_candidates_kernel, edge_kernel: the edge pass.  A point-sampled frame
-// has no derivative with respect to r_out, and its derivatives with respect
-// to the spin and the inclination miss the motion of the disc's edges; the
-// derivative of the frame averaged over each sample's cell has both.  Each
+// The edge pass: a point-sampled frame has no derivative with respect to
+// r_out, and its derivatives with respect to the spin and the inclination
+// miss the motion of the disc's edges; the derivative of the frame averaged
+// over each sample's cell has both.  edge_candidates_kernel picks each
 // sample's first two equatorial crossings near an edge (adj::edge_mask,
-// against the spread of the neighbouring samples' same crossing) get the
-// edge term of adj::edge_sample with weight 2 (Y_pixel - target).
+// against the spread of the neighbouring samples' same crossing; the render
+// records the crossings), and the adjoint kernel takes their edge terms
+// (adj::edge_sample, weight 2 (Y_pixel - target)) as its first jobs, so the
+// long ones overlap the per-ray work instead of forming a tail of their own.
 //
 // The edge pass covers the edges of the first two equatorial crossings (the
 // direct image of the disc and its first lensed image).  Images of order
@@ -37,6 +39,51 @@ namespace {
 constexpr int kAdjBlock = 128;
 constexpr int kReduceThreads = 1024;
 
+// Candidate selection: one thread per sample (work order); each of its first
+// two equatorial crossings, as the render recorded them, is compared with the
+// same crossing of its four neighbours in the W S x H S sample grid
+// (adj::edge_mask).
+__global__ void __launch_bounds__(256) edge_candidates_kernel(const AdjointLaunch L) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= L.n_rays) return;
+    const int S = L.frame.S;
+    const int SS = S * S;
+    const int W = L.frame.width, H = L.frame.height;
+    const long long pixel = id / SS;
+    const int k = (int)(id - pixel * SS);
+    int px, py;
+    pixel_xy(W, H, pixel, &px, &py);
+    const int gx = px * S + k % S;
+    const int gy = py * S + k / S;
+    const int GW = W * S, GH = H * S;
+    for (int j = 0; j < 2; ++j) {
+        const double rc = L.xing_r[2 * id + j];
+        if (rc == 0.0) break;
+        double dmax = 0.0;
+        #pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int nx = gx + (n == 0) - (n == 1);
+            const int ny = gy + (n == 2) - (n == 3);
+            if (nx < 0 || nx >= GW || ny < 0 || ny >= GH) continue;
+            const long long nid = pixel_index(W, H, nx / S, ny / S) * SS + (ny % S) * S + nx % S;
+            const double rn = L.xing_r[2 * nid + j];
+            if (rn == 0.0) continue;
+            const double d = fabs(rc - rn);
+            if (d > dmax) dmax = d;
+        }
+        const int m = adj::edge_mask(L.frame, rc, dmax);
+        if (m) {
+            const unsigned long long at = atomicAdd(&L.counters[6], 1ull);
+            L.cand[at] = ((unsigned long long)(2 * id + j) << 2) | (unsigned long long)m;
+        }
+    }
+}
+
+// One queue of jobs: first the edge candidates (each a forward pass to its
+// crossing, the continuation past it and a reverse sweep: the longest jobs),
+// then the rays.  Each thread owns `checkpoint_slots` checkpoint states for
+// the job it is working on; results go to per-ray and per-crossing slots, so
+// the sums do not depend on which thread took which job.
 __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const AdjointLaunch L) {
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int slots = L.X.checkpoint_slots;
@@ -44,9 +91,32 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const AdjointLaunch 
     const int S = L.frame.S;
     const int SS = S * S;
     const int W = L.frame.width, H = L.frame.height;
+    const unsigned long long n_cand = L.counters[6];
     unsigned long long steps = 0, replay = 0, disc = 0, sky = 0, max_int = 0, n_high = 0;
+    unsigned long long edge_steps = 0, edge_cells = 0;
     for (;;) {
-        const long long id = (long long)atomicAdd(&L.counters[0], 1ull);
+        const unsigned long long job = atomicAdd(&L.counters[0], 1ull);
+        if (job < n_cand) {
+            const unsigned long long c = L.cand[job];
+            const long long xs = (long long)(c >> 2);     // 2 * ray + crossing
+            const long long id = xs >> 1;
+            const long long pixel = id / SS;
+            const int k = (int)(id - pixel * SS);
+            int px, py;
+            pixel_xy(W, H, pixel, &px, &py);
+            const long long pix = (long long)py * W + px;
+            const double w = 2.0 * (L.pixels[pix].y - (double)L.target[pix]);
+            double out[3];
+            int n_cells = 0;
+            edge_steps += (unsigned long long)adj::edge_sample(L.frame, L.X, L.sky, px, py, k, (int)(xs & 1) + 1,
+                                                               (int)(c & 3ull), w, ck, slots, out, &n_cells);
+            edge_cells += (unsigned long long)n_cells;
+            L.edge_out[3 * xs] = out[0];
+            L.edge_out[3 * xs + 1] = out[1];
+            L.edge_out[3 * xs + 2] = out[2];
+            continue;
+        }
+        const long long id = (long long)(job - n_cand);
         if (id >= L.n_rays) break;
         const long long pixel = id / SS;
         const int k = (int)(id - pixel * SS);
@@ -62,10 +132,6 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const AdjointLaunch 
         xr.step[0] = xr.step[1] = 0;
         adj::adjoint_ray(L.frame, L.X, L.sky, id, w, ck, slots, false, &res, &xr);
         const long long o = pix * SS + k;
-        L.xing_r[2 * o] = xr.r[0];
-        L.xing_r[2 * o + 1] = xr.r[1];
-        L.xing_step[2 * o] = xr.step[0];
-        L.xing_step[2 * o + 1] = xr.step[1];
         const bool high = xr.count >= 3 && (res.what == BH_HIT_DISC || res.what == BH_HIT_SKY);
         L.high_order[o] = high ? 1 : 0;
         n_high += high ? 1ull : 0ull;
@@ -83,79 +149,9 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const AdjointLaunch 
     atomicAdd(&L.counters[3], disc);
     atomicAdd(&L.counters[4], sky);
     atomicMax(&L.counters[5], max_int);
-    atomicAdd(&L.counters[10], n_high);
-}
-
-// Candidate selection: one thread per sample; each of its first two
-// equatorial crossings is compared with the same crossing of its four
-// neighbours in the W S x H S sample grid (adj::edge_mask).
-__global__ void __launch_bounds__(256) edge_candidates_kernel(const AdjointLaunch L) {
-    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= L.n_rays) return;
-    const int S = L.frame.S;
-    const int SS = S * S;
-    const long long pix = o / SS;
-    const int k = (int)(o - pix * SS);
-    const int W = L.frame.width, H = L.frame.height;
-    const int gx = (int)(pix % W) * S + k % S;
-    const int gy = (int)(pix / W) * S + k / S;
-    const int GW = W * S, GH = H * S;
-    for (int j = 0; j < 2; ++j) {
-        if (L.xing_step[2 * o + j] == 0) break;
-        const double rc = L.xing_r[2 * o + j];
-        double dmax = 0.0;
-        #pragma unroll
-        for (int n = 0; n < 4; ++n) {
-            const int nx = gx + (n == 0) - (n == 1);
-            const int ny = gy + (n == 2) - (n == 3);
-            if (nx < 0 || nx >= GW || ny < 0 || ny >= GH) continue;
-            const long long on = ((long long)(ny / S) * W + nx / S) * SS + (ny % S) * S + nx % S;
-            if (L.xing_step[2 * on + j] == 0) continue;
-            const double d = fabs(rc - L.xing_r[2 * on + j]);
-            if (d > dmax) dmax = d;
-        }
-        const int m = adj::edge_mask(L.frame, rc, dmax);
-        if (m) {
-            const unsigned long long at = atomicAdd(&L.counters[6], 1ull);
-            L.cand[at] = ((unsigned long long)(2 * o + j) << 2) | (unsigned long long)m;
-        }
-    }
-}
-
-// The edge term of each candidate; candidates handed out by an atomic
-// counter, each thread with its own checkpoint slots, results written per
-// crossing slot so the sums do not depend on the order.
-__global__ void __launch_bounds__(kAdjBlock) edge_kernel(const AdjointLaunch L) {
-    const long long thread = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int slots = L.X.checkpoint_slots;
-    double* ck = L.ckpt + thread * slots * 8;
-    const unsigned long long n_cand = L.counters[6];
-    const int S = L.frame.S;
-    const int SS = S * S;
-    const int W = L.frame.width;
-    unsigned long long steps = 0, cells = 0;
-    for (;;) {
-        const unsigned long long i = atomicAdd(&L.counters[7], 1ull);
-        if (i >= n_cand) break;
-        const unsigned long long c = L.cand[i];
-        const long long slot = (long long)(c >> 2);
-        const int edges = (int)(c & 3ull);
-        const long long o = slot >> 1;
-        const long long pix = o / SS;
-        const int k = (int)(o - pix * SS);
-        const int px = (int)(pix % W), py = (int)(pix / W);
-        const double w = 2.0 * (L.pixels[pix].y - (double)L.target[pix]);
-        double out[3];
-        int n_cells = 0;
-        steps += (unsigned long long)adj::edge_sample(L.frame, L.X, L.sky, px, py, k, L.xing_step[slot], edges, w,
-                                                      ck, slots, out, &n_cells);
-        cells += (unsigned long long)n_cells;
-        L.edge_out[3 * slot] = out[0];
-        L.edge_out[3 * slot + 1] = out[1];
-        L.edge_out[3 * slot + 2] = out[2];
-    }
-    atomicAdd(&L.counters[8], steps);
-    atomicAdd(&L.counters[9], cells);
+    atomicAdd(&L.counters[7], edge_steps);
+    atomicAdd(&L.counters[8], edge_cells);
+    atomicAdd(&L.counters[9], n_high);
 }
 
 __global__ void __launch_bounds__(kReduceThreads)
@@ -202,9 +198,8 @@ int adjoint_blocks_per_sm(int block_size) {
 cudaError_t launch_adjoint(const AdjointLaunch& L, cudaStream_t stream) {
     if (L.block != kAdjBlock) return cudaErrorInvalidValue;
     if (L.n_rays > 0) {
-        adjoint_kernel<<<L.grid, L.block, 0, stream>>>(L);
         edge_candidates_kernel<<<(unsigned)((L.n_rays + 255) / 256), 256, 0, stream>>>(L);
-        edge_kernel<<<L.grid, L.block, 0, stream>>>(L);
+        adjoint_kernel<<<L.grid, L.block, 0, stream>>>(L);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -824,17 +824,19 @@ struct Crossings {
 };
 
 // Integrates from `s` with the render path's events (render.cpp:158-257)
-// until the ray ends, returning its class, or until accepted step `stop_at`
-// has been taken, returning -1 before that step's events are looked at.  The
-// crossing radius of a disc hit goes to *r_hit.  Checkpoints (cp) and the
-// first two equatorial crossings (xr) are recorded when given.
+// until the ray ends, returning its class, or until its equatorial crossing
+// number `stop_crossing` (counted from `s`; 0: none), returning -1 after that
+// crossing's step with its radius in *r_hit and without looking at whether
+// it hits the disc.  The crossing radius of a disc hit goes to *r_hit.
+// Checkpoints (cp) and the first two equatorial crossings (xr) are recorded
+// when given.
 __host__ __device__ inline int forward_run(const FrameParams& F, const RayC& c, Integ& s, Checkpoints* cp,
-                                           Crossings* xr, int stop_at, double* r_hit) {
+                                           Crossings* xr, int stop_crossing, double* r_hit) {
     if (F.max_steps <= 0) return BH_HIT_EXHAUSTED;
     StepRec rec;
+    int crossings = 0;
     for (;;) {
         if (!advance(F, c, s, &rec)) return BH_HIT_HORIZON;   // no acceptable step (render.cpp:133-136)
-        if (s.steps == stop_at) return -1;
         const double rn = rec.yn[1];
         if (rn <= F.r_stop) return BH_HIT_HORIZON;
         if (F.disc_enabled && rec.c0 * rec.c7 < 0.0) {
@@ -850,6 +852,10 @@ __host__ __device__ inline int forward_run(const FrameParams& F, const RayC& c, 
                     xr->step[xr->n++] = s.steps;
                 }
                 ++xr->count;
+            }
+            if (++crossings == stop_crossing) {
+                *r_hit = rc;
+                return -1;
             }
             if (rc >= F.r_in && rc <= F.r_out) {
                 *r_hit = rc;
@@ -944,7 +950,7 @@ __host__ __device__ inline void adjoint_ray(const FrameParams& F, const AdjointF
     Checkpoints cp{ck, slots, X.checkpoint_interval, 0};
     cp.push(s);
     double r_hit = 0.0;
-    const int what = forward_run(F, c, s, &cp, xr, -1, &r_hit);
+    const int what = forward_run(F, c, s, &cp, xr, 0, &r_hit);
     out->what = what;
     out->steps = s.steps;
     out->interval = cp.interval;
@@ -1068,7 +1074,7 @@ __host__ __device__ inline double line_in_cell(double gx, double gy, double cx, 
 // Edges of the disc an equatorial crossing can be near.
 enum { kEdgeOuter = 1, kEdgeInner = 2 };
 
-// The edge term of the equatorial crossing in accepted step `step` of sample k
+// The edge term of equatorial crossing number `crossing` (1 or 2) of sample k
 // of pixel (px, py), for the disc edges in `edges` (kEdgeOuter: r_out;
 // kEdgeInner: r_in, the ISCO) and pixel weight w = dLoss/d(pixel).  With
 // phi = r_out - r_c (outer) or r_c - r_in (inner), positive on the disc side,
@@ -1079,9 +1085,10 @@ enum { kEdgeOuter = 1, kEdgeInner = 2 };
 // inclination), d r_c/d(su, sv), and per edge (outer, inner) L and
 // Y_disc - Y_beyond.  Returns the accepted steps integrated (forward,
 // continuation and replay).
-__host__ __device__ inline long long edge_sample(const FrameParams& F, const AdjointFrame& X, const SkyData& sky,
-                                                 int px, int py, int k, int step, int edges, double w, double* ck,
-                                                 int slots, double out[3], int* cells, double* diag = nullptr) {
+__host__ __device__ BHA_NOINLINE long long edge_sample(const FrameParams& F, const AdjointFrame& X, const SkyData& sky,
+                                                 int px, int py, int k, int crossing, int edges, double w,
+                                                 double* ck, int slots, double out[3], int* cells,
+                                                 double* diag = nullptr) {
     out[0] = out[1] = out[2] = 0.0;
     *cells = 0;
     double su, sv, xp, yp;
@@ -1093,13 +1100,15 @@ __host__ __device__ inline long long edge_sample(const FrameParams& F, const Adj
     integ_start(F, y0, s);
     Checkpoints cp{ck, slots, X.checkpoint_interval, 0};
     cp.push(s);
-    double r_hit = 0.0;
-    if (forward_run(F, c, s, &cp, nullptr, step, &r_hit) != -1) return s.steps;
+    double rc = 0.0;
+    if (forward_run(F, c, s, &cp, nullptr, crossing, &rc) != -1) return s.steps;
+    const int step = s.steps;
 
-    // What the ray meets when the crossing of that step misses the disc: its
+    // What the ray meets when this crossing misses the disc: its
     // continuation traced on from there.
     Integ t = s;
-    const int what = forward_run(F, c, t, nullptr, nullptr, -1, &r_hit);
+    double r_hit = 0.0;
+    const int what = forward_run(F, c, t, nullptr, nullptr, 0, &r_hit);
     long long work = t.steps;
     double Y_beyond = 0.0;
     if (what == BH_HIT_DISC) {
@@ -1118,29 +1127,6 @@ __host__ __device__ inline long long edge_sample(const FrameParams& F, const Adj
                           (edges & kEdgeInner) ? -Y_beyond : 0.0};
     if (dY[0] == 0.0 && dY[1] == 0.0 && !diag) return work;
 
-    // the crossing radius of that step, as the forward pass found it
-    double rc;
-    {
-        const int seg = (step - 1) / cp.interval;
-        const double* p = cp.ck + 8 * seg;
-        Integ r;
-        for (int i = 0; i < 6; ++i) r.y[i] = p[i];
-        r.h = p[6];
-        r.err_prev = p[7];
-        r.have_k1 = 0;
-        r.tries = 0;
-        r.steps = seg * cp.interval;
-        StepRec q;
-        while (r.steps < step) advance(F, c, r, &q);
-        work += step - seg * cp.interval;
-        if (!(q.c0 * q.c7 < 0.0)) return work;   // not a crossing step: nothing to differentiate
-        const DenseC cth = dense_coef(q.h, q.y[2], q.yn[2], q.kth[0], q.kth[2], q.kth[3], q.kth[4], q.kth[5],
-                                      q.kth[6]);
-        const double s_end = dense_crossing(cth, crossing_target(cth.r1, cth.r1 + cth.r2));
-        const DenseC crr = dense_coef(q.h, q.y[1], q.yn[1], q.kr[0], q.kr[2], q.kr[3], q.kr[4], q.kr[5],
-                                      q.kr[6]);
-        rc = dense_eval(crr, s_end);
-    }
     // d r_c / d(initial state, E, L_z, spin) by a reverse sweep seeded with r_c
     double yb[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     double Eb = 0.0, Lzb = 0.0, ab = 0.0;

@@ -53,18 +53,18 @@ struct AdjointLaunch {
     double* ray_Y;                   // luminance per ray in the same order, or nullptr
     double* ckpt;                    // grid * block * checkpoint_slots * 8 doubles
     // The edge pass: per crossing slot (2 per ray, slot = 2 * ray + crossing,
-    // rays in ray_grad order) the radius and accepted step of the ray's first
-    // two equatorial crossings (step 0: none), the candidate list
-    // ((slot << 2) | kEdge* bits) and 3 edge contributions per slot.
+    // rays in work order) the radius of the ray's first two equatorial
+    // crossings as the render found them (0: none; zeroed before the
+    // render), the candidate list ((slot << 2) | kEdge* bits) and 3 edge
+    // contributions per slot.
     double* xing_r;
-    int* xing_step;
     unsigned long long* cand;
     double* edge_out;
     // 1 for a ray whose event came after its third or later equatorial
     // crossing (an image of order three or higher), in ray_grad order
     unsigned char* high_order;
-    // next ray, accepted, replayed, disc rays, sky rays, max interval, edge
-    // candidates, next candidate, edge-pass steps, edge cells, high-order rays
+    // next job, accepted, replayed, disc rays, sky rays, max interval, edge
+    // candidates, edge-pass steps, edge cells, high-order rays
     unsigned long long* counters;
     // loss; the four per-ray gradient sums (spin and inclination over the
     // rays of image order one and two); the three edge sums; the spin and
@@ -74,13 +74,13 @@ struct AdjointLaunch {
     int grid, block;
 };
 
-constexpr int kAdjCounters = 11;
+constexpr int kAdjCounters = 10;
 constexpr int kAdjSums = 10;
 
-// Enqueues the adjoint kernel, the edge pass (candidate selection over the
-// sample grid, then the edge term of each candidate) and the deterministic
-// reduction of the per-ray gradients, the edge contributions and the loss;
-// `counters` and `edge_out` must be zeroed before.
+// Enqueues the edge pass's candidate selection over the sample grid, the
+// adjoint kernel (edge terms, then the rays) and the deterministic reduction
+// of the per-ray gradients, the edge contributions and the loss; `counters`
+// and `edge_out` must be zeroed before.
 cudaError_t launch_adjoint(const AdjointLaunch& L, cudaStream_t stream);
 // Resident blocks of the adjoint kernel per SM at `block_size` threads.
 int adjoint_blocks_per_sm(int block_size);

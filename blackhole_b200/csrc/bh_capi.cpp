@@ -62,7 +62,7 @@ struct bh_ctx {
     DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats, deferred, jet;
     // Adjoint: target image, per-ray gradients and luminances, checkpoint
     // slots, counters and the five sums.
-    DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums, adj_xr, adj_xs, adj_cand, adj_edge, adj_high;
+    DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums, adj_xr, adj_cand, adj_edge, adj_high;
     // Display transform: blur scratch, glare weights, meter state, 8-bit output.
     DevBuf disp_tmp, disp_near, disp_far, disp_k, disp_state, disp_rgb;
     QueueState* d_queue = nullptr;
@@ -475,8 +475,8 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end, &ctx->deferred,
                       &ctx->pix_end, &ctx->partials, &ctx->fstats, &ctx->jet, &ctx->adj_target, &ctx->adj_grad, &ctx->adj_Y,
-                      &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums, &ctx->adj_xr, &ctx->adj_xs, &ctx->adj_cand,
-                      &ctx->adj_edge, &ctx->adj_high, &ctx->disp_tmp, &ctx->disp_near,
+                      &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums, &ctx->adj_xr, &ctx->adj_cand, &ctx->adj_edge,
+                      &ctx->adj_high, &ctx->disp_tmp, &ctx->disp_near,
                       &ctx->disp_far, &ctx->disp_k, &ctx->disp_state, &ctx->disp_rgb})
         if (b->p) cudaFree(b->p);
     cudaFree(ctx->d_table);
@@ -678,16 +678,23 @@ static int adjoint_impl(bh_ctx* ctx, const bh_render_config* cfg, const float* t
     if ((rc = ensure(ctx, ctx->adj_sums, kAdjSums * sizeof(double))) != BH_OK) return rc;
     const size_t n_slots = static_cast<size_t>(n_rays) * 2;     // two equatorial crossings per ray
     if ((rc = ensure(ctx, ctx->adj_xr, n_slots * sizeof(double))) != BH_OK) return rc;
-    if ((rc = ensure(ctx, ctx->adj_xs, n_slots * sizeof(int))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->adj_cand, n_slots * sizeof(unsigned long long))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->adj_edge, n_slots * 3 * sizeof(double))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->adj_high, static_cast<size_t>(n_rays))) != BH_OK) return rc;
 
     CK(cudaMemcpyAsync(ctx->adj_target.p, target, npx * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     ctx->h2d += static_cast<long long>(npx * sizeof(float));
+    CK(cudaMemsetAsync(ctx->adj_xr.p, 0, n_slots * sizeof(double), ctx->stream));
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    if ((rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, false)) != BH_OK)
-        return rc;
+    {
+        // the render, recording each ray's first two equatorial crossings
+        Plan p;
+        if ((rc = plan_launch(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, false, p)) != BH_OK)
+            return rc;
+        p.tl.xing = static_cast<double*>(ctx->adj_xr.p);
+        ctx->h2d += static_cast<long long>(p.stage_bytes);
+        if ((rc = record_launch(ctx, p, ctx->stream, false)) != BH_OK) return rc;
+    }
     CK(cudaMemsetAsync(ctx->adj_counters.p, 0, kAdjCounters * sizeof(unsigned long long), ctx->stream));
     CK(cudaMemsetAsync(ctx->adj_edge.p, 0, n_slots * 3 * sizeof(double), ctx->stream));
     AdjointLaunch L;
@@ -701,7 +708,6 @@ static int adjoint_impl(bh_ctx* ctx, const bh_render_config* cfg, const float* t
     L.ray_Y = ray_Y ? static_cast<double*>(ctx->adj_Y.p) : nullptr;
     L.ckpt = static_cast<double*>(ctx->adj_ckpt.p);
     L.xing_r = static_cast<double*>(ctx->adj_xr.p);
-    L.xing_step = static_cast<int*>(ctx->adj_xs.p);
     L.cand = static_cast<unsigned long long*>(ctx->adj_cand.p);
     L.edge_out = static_cast<double*>(ctx->adj_edge.p);
     L.high_order = static_cast<unsigned char*>(ctx->adj_high.p);
@@ -736,11 +742,11 @@ static int adjoint_impl(bh_ctx* ctx, const bh_render_config* cfg, const float* t
     out->edge_spin = sums[6];
     out->edge_inclination = sums[7];
     out->edge_candidates = static_cast<long long>(cnt[6]);
-    out->edge_steps = static_cast<long long>(cnt[8]);
-    out->edge_cells = static_cast<long long>(cnt[9]);
+    out->edge_steps = static_cast<long long>(cnt[7]);
+    out->edge_cells = static_cast<long long>(cnt[8]);
     out->held_spin = sums[8];
     out->held_inclination = sums[9];
-    out->high_order_rays = static_cast<long long>(cnt[10]);
+    out->high_order_rays = static_cast<long long>(cnt[9]);
     out->kernel_ms = ms;
     out->rays = n_rays;
     out->steps = static_cast<long long>(cnt[1]);

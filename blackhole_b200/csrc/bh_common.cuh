@@ -39,6 +39,14 @@ __host__ __device__ __forceinline__ void pixel_xy(int W, int H, long long p, int
     *y = y0 + rel % bh;
 }
 
+// The inverse of pixel_xy: the frame-local pixel index of pixel (x, y).
+__host__ __device__ __forceinline__ long long pixel_index(int W, int H, int x, int y) {
+    const int band = y >> 2;
+    const int y0 = 4 * band;
+    const int bh = (H - y0 < 4) ? H - y0 : 4;
+    return (long long)band * 4 * W + (long long)x * bh + (y - y0);
+}
+
 // Index of the frame whose cumulative end exceeds `id` (ends ascending).
 __device__ __forceinline__ int find_frame(const long long* __restrict__ ends, int n, long long id) {
     int lo = 0, hi = n - 1;

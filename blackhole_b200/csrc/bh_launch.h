@@ -31,6 +31,8 @@ struct TraceLaunch {
     cudaEvent_t resume_event;        // recorded between the two launches (optional)
     double* jet;                     // jet emission per ray (total_rays), or null when no
                                      // frame of the launch has a jet
+    double* xing;                    // radii of each ray's first two equatorial crossings
+                                     // (2 per ray, zeroed before; 0 = none), or null
 };
 
 // Bytes of one deferred-ray record.

@@ -267,6 +267,7 @@ struct TraceArgs {
     int refill;
     unsigned long long budget;
     double* jet;             // jet emission per ray (jet kernels only)
+    double* xing;            // first two equatorial crossing radii per ray, or null
 };
 
 template <class P>
@@ -501,6 +502,12 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         const double s_end = dense_crossing(cth, 0.5 * kPi + m * kPi);
         const DenseC crr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
         const double rc = dense_eval(crr, s_end);
+        if (A.xing) {
+            // the crossings the discrete adjoint's edge pass starts from
+            double* x = A.xing + 2 * L.gid;
+            if (x[0] == 0.0) x[0] = rc;
+            else if (x[1] == 0.0) x[1] = rc;
+        }
         if (rc >= F.r_in && rc <= F.r_out) {
             what = BH_HIT_DISC;
             s_jet = s_end;
@@ -744,6 +751,7 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.refill = L.refill < 1 ? 1 : (L.refill > 32 ? 32 : L.refill);
     A.budget = L.budget;
     A.jet = L.jet;
+    A.xing = L.xing;
     trace_kernel<P, MAXREG, JET><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
 }

@@ -169,14 +169,15 @@ int bhx_crossings(const bh_render_config* cfg, long long local_id, double r[2], 
     return BH_OK;
 }
 
-// The edge term (edge_sample) of the crossing in accepted step `step` of
-// sample k of pixel (px, py) for the edges `edges` (1 outer, 2 inner, 3 both):
+// The edge term (edge_sample) of equatorial crossing number `crossing` (1 or
+// 2) of sample k of pixel (px, py) for the edges `edges` (1 outer, 2 inner,
+// 3 both):
 // out = contributions to dLoss/d(r_out, spin, inclination) for pixel weight
 // w; diag = (r_c, |grad r_c|, d r_c/d spin, d r_c/d incl, d r_c/d su,
 // d r_c/d sv, L and dY of the outer edge, L and dY of the inner edge, cells
 // crossed, steps integrated).
-int bhx_edge(const bh_render_config* cfg, int px, int py, int k, int step, int edges, double w, double out[3],
-             double diag[12]) {
+int bhx_edge(const bh_render_config* cfg, int px, int py, int k, int crossing, int edges, double w,
+             double out[3], double diag[12]) {
     std::lock_guard<std::mutex> lock(g_mu);
     FrameParams F;
     AdjointFrame X;
@@ -187,7 +188,8 @@ int bhx_edge(const bh_render_config* cfg, int px, int py, int k, int step, int e
     for (int i = 0; i < 12; ++i) diag[i] = 0.0;
     int cells = 0;
     diag[11] = static_cast<double>(
-        adj::edge_sample(F, X, sd, px, py, k, step, edges, w, ck.data(), X.checkpoint_slots, out, &cells, diag));
+        adj::edge_sample(F, X, sd, px, py, k, crossing, edges, w, ck.data(), X.checkpoint_slots, out, &cells,
+                         diag));
     diag[10] = cells;
     return BH_OK;
 }
@@ -217,9 +219,9 @@ int bhx_sample_position(const bh_render_config* cfg, int px, int py, int k, doub
     return BH_OK;
 }
 
-// The equatorial-crossing radius at accepted step `step` of the ray through
-// image-plane position (su, sv), or NaN when the ray ends before that step.
-int bhx_crossing_radius(const bh_render_config* cfg, double su, double sv, int step, double* r_c) {
+// The radius of equatorial crossing number `crossing` of the ray through
+// image-plane position (su, sv), or NaN when the ray ends before it.
+int bhx_crossing_radius(const bh_render_config* cfg, double su, double sv, int crossing, double* r_c) {
     std::lock_guard<std::mutex> lock(g_mu);
     FrameParams F;
     AdjointFrame X;
@@ -231,18 +233,8 @@ int bhx_crossing_radius(const bh_render_config* cfg, double su, double sv, int s
     const adj::RayC c = adj::ray_consts(F, E, Lz);
     adj::Integ s;
     adj::integ_start(F, y0, s);
-    double r_hit = 0.0;
-    *r_c = std::nan("");
-    if (step > 1 && adj::forward_run(F, c, s, nullptr, nullptr, step - 1, &r_hit) != -1) return BH_OK;
-    adj::StepRec q;
-    if (!adj::advance(F, c, s, &q)) return BH_OK;
-    if (q.c0 * q.c7 >= 0.0) return BH_OK;
-    const DenseC cth = dense_coef(q.h, q.y[2], q.yn[2], q.kth[0], q.kth[2], q.kth[3], q.kth[4],
-                                            q.kth[5], q.kth[6]);
-    const double s_end = dense_crossing(cth, adj::crossing_target(cth.r1, cth.r1 + cth.r2));
-    const DenseC crr = dense_coef(q.h, q.y[1], q.yn[1], q.kr[0], q.kr[2], q.kr[3], q.kr[4], q.kr[5],
-                                            q.kr[6]);
-    *r_c = dense_eval(crr, s_end);
+    double r = 0.0;
+    *r_c = (adj::forward_run(F, c, s, nullptr, nullptr, crossing, &r) == -1) ? r : std::nan("");
     return BH_OK;
 }
 

@@ -214,17 +214,17 @@ def _crossings(lib, cfg):
     return R, ST
 
 
-def _edge(lib, cfg, px, py, k, step, edges, w=1.0):
+def _edge(lib, cfg, px, py, k, crossing, edges, w=1.0):
     out, diag = _a(np.zeros(3)), _a(np.zeros(12))
     c = cfg.to_c()
-    assert lib.bhx_edge(C.byref(c), px, py, k, step, edges, w, _p(out), _p(diag)) == abi.OK
+    assert lib.bhx_edge(C.byref(c), px, py, k, crossing, edges, w, _p(out), _p(diag)) == abi.OK
     return out, diag
 
 
-def _rc(lib, cfg, su, sv, step):
+def _rc(lib, cfg, su, sv, crossing):
     c = cfg.to_c()
     r = C.c_double()
-    assert lib.bhx_crossing_radius(C.byref(c), su, sv, step, C.byref(r)) == abi.OK
+    assert lib.bhx_crossing_radius(C.byref(c), su, sv, crossing, C.byref(r)) == abi.OK
     return r.value
 
 
@@ -239,7 +239,7 @@ def edge_frame(chk):
 def test_crossing_radius_gradient_matches_finite_differences(chk, edge_frame):
     """d r_c/d(su, sv, spin, inclination) from the reverse sweep of the
     crossing radius, at crossings next to both edges, against central
-    differences of the crossing radius of the same accepted step."""
+    differences of the radius of the same crossing."""
     cfg, R, ST = edge_frame
     r_in = _isco(cfg.spin)
     picked = []
@@ -249,7 +249,7 @@ def test_crossing_radius_gradient_matches_finite_differences(chk, edge_frame):
         picked += [(edge, int(o), int(j)) for o, j in near[:: max(1, len(near) // 3)][:3]]
     for edge, o, j in picked:
         px, py = o % cfg.width, o // cfg.width
-        step = int(ST[o, j])
+        step = j + 1                  # crossing number
         _, diag = _edge(chk, cfg, px, py, 0, step, edge)
         assert diag[0] == pytest.approx(R[o, j], rel=1e-12)
         pos = _a(np.zeros(4))
@@ -279,7 +279,7 @@ def test_edge_term_of_a_cell_is_the_swept_area(chk, edge_frame):
     seen = 0
     for o, j in near:
         px, py = int(o) % cfg.width, int(o) // cfg.width
-        out, d = _edge(chk, cfg, px, py, 0, int(ST[o, j]), 1, w=3.0)
+        out, d = _edge(chk, cfg, px, py, 0, int(j) + 1, 1, w=3.0)
         rc, gn, drq, L, dY = d[0], d[1], d[2:4], d[6], d[7]
         if L == 0.0 or dY == 0.0:
             assert not out.any()
@@ -319,7 +319,7 @@ def test_candidate_rule_finds_every_cell_an_edge_crosses(chk, edge_frame):
             for bit, re, ok in ((1, cfg.disc_r_out, rc >= r_in), (2, r_in, rc <= cfg.disc_r_out)):
                 if not ok or abs(rc - re) > 0.25 * re:
                     continue
-                _, d = _edge(chk, cfg, x, y, 0, int(ST[o, j]), bit)
+                _, d = _edge(chk, cfg, x, y, 0, j + 1, bit)
                 if d[6 if bit == 1 else 8] > 0.0:
                     crossed += 1
                     assert m.value & bit, (o, j, bit, rc, dmax)
