@@ -391,7 +391,8 @@ def animation_leg(r, frames=48, width=512, height=288):
 def adjoint_leg(r, steps=3, warmup=1):
     """Gradients per second of the discrete adjoint on the 512^2 gradient
     workload: one gradient = the binary64 render, the loss against the target
-    frame and d(loss)/d(spin, inclination, Eddington ratio, r_out)."""
+    frame and d(loss)/d(spin, inclination, Eddington ratio, r_out), the
+    disc-edge term included."""
     from blackhole_b200 import workloads
 
     cfg = workloads.adjoint_512()
@@ -415,7 +416,12 @@ def adjoint_leg(r, steps=3, warmup=1):
             "loss": gs["loss"], "grad": [gs["d_spin"], gs["d_inclination"], gs["d_eddington"], gs["d_r_out"]],
             "steps_per_ray": round(gs["steps"] / gs["rays"], 2),
             "replay_over_forward": round(gs["replayed_steps"] / max(1, gs["steps"]), 3),
-            "disc_rays": gs["disc_rays"], "sky_rays": gs["sky_rays"]}
+            "disc_rays": gs["disc_rays"], "sky_rays": gs["sky_rays"],
+            "edge": {"candidates": gs["edge_candidates"], "cells": gs["edge_cells"],
+                     "steps_over_forward": round(gs["edge_steps"] / max(1, gs["steps"]), 3),
+                     "d_spin": gs["edge_spin"], "d_inclination": gs["edge_inclination"]},
+            "held_out": {"rays": gs["high_order_rays"], "d_spin": gs["held_spin"],
+                         "d_inclination": gs["held_inclination"]}}
 
 
 def ring_adjoint_leg(r, steps=2):
@@ -436,7 +442,10 @@ def ring_adjoint_leg(r, steps=2):
                         "critical-curve centre), binary64; target at a=0.99, 76 deg",
             "value": round(1e3 / m, 2), "unit": "grads/s", "ms_per_grad": round(m, 3),
             "grad": [g["d_spin"], g["d_inclination"]], "loss": g["loss"],
-            "steps_per_ray": round(g["steps"] / g["rays"], 2)}
+            "steps_per_ray": round(g["steps"] / g["rays"], 2),
+            "edge": {"candidates": g["edge_candidates"], "cells": g["edge_cells"]},
+            "held_out": {"rays": g["high_order_rays"], "d_spin": g["held_spin"],
+                         "d_inclination": g["held_inclination"]}}
 
 
 def autotune_leg():
