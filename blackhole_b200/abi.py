@@ -35,6 +35,7 @@ STATUS_NAMES = {
 HIT_HORIZON, HIT_DISC, HIT_SUN, HIT_STAR, HIT_SKY, HIT_EXHAUSTED = range(6)
 # Display tone curves, in img::ToneMap order (image.h:16).
 TONEMAP_LINEAR, TONEMAP_REINHARD, TONEMAP_ACES, TONEMAP_LOG, TONEMAP_HDR = range(5)
+EVAL_RHS, EVAL_DISC_TEMPERATURE, EVAL_BLACKBODY, EVAL_FRAME = range(4)
 TONEMAP_NAMES = ("linear", "reinhard", "aces", "log", "hdr")
 HIT_NAMES = ("Horizon", "Disc", "Sun", "Star", "Sky", "Exhausted")
 

@@ -61,10 +61,12 @@ struct bh_ctx {
 
     DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats, deferred, jet;
     // Adjoint: target image, per-ray gradients and luminances, checkpoint
-    // slots, counters and the five sums.
+    // slots, counters, sums and the edge pass's buffers.
     DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums, adj_xr, adj_cand, adj_edge, adj_high;
     // Display transform: blur scratch, glare weights, meter state, 8-bit output.
     DevBuf disp_tmp, disp_near, disp_far, disp_k, disp_state, disp_rgb;
+    // bh_gpu_eval: inputs and outputs.
+    DevBuf eval_in, eval_out;
     QueueState* d_queue = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     long long h2d = 0, d2h = 0;          // bytes copied by the current call
@@ -476,7 +478,7 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     for (DevBuf* b : {&ctx->hits, &ctx->pixels, &ctx->rays, &ctx->lum, &ctx->frames, &ctx->ray_end, &ctx->deferred,
                       &ctx->pix_end, &ctx->partials, &ctx->fstats, &ctx->jet, &ctx->adj_target, &ctx->adj_grad, &ctx->adj_Y,
                       &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums, &ctx->adj_xr, &ctx->adj_cand, &ctx->adj_edge,
-                      &ctx->adj_high, &ctx->disp_tmp, &ctx->disp_near,
+                      &ctx->adj_high, &ctx->eval_in, &ctx->eval_out, &ctx->disp_tmp, &ctx->disp_near,
                       &ctx->disp_far, &ctx->disp_k, &ctx->disp_state, &ctx->disp_rgb})
         if (b->p) cudaFree(b->p);
     cudaFree(ctx->d_table);
@@ -905,6 +907,48 @@ int bh_gpu_render_batch_rgb(bh_ctx* ctx, const bh_render_config* cfgs, int n, co
     }
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return finish(ctx, n, stats, nullptr, true, secs);
+}
+
+int bh_gpu_eval(bh_ctx* ctx, const bh_render_config* cfg, int what, const double* in, long long n, double* out) {
+    if (!ctx) return BH_ERR_INVALID_ARG;
+    if (!out || n < 0 || (n > 0 && !in && what != BH_EVAL_FRAME))
+        return fail(ctx, BH_ERR_INVALID_ARG, "in/out must not be NULL and n must be >= 0");
+    if (what < BH_EVAL_RHS || what > BH_EVAL_FRAME) return fail(ctx, BH_ERR_INVALID_ARG, "unknown evaluation");
+    CK(cudaSetDevice(ctx->device));
+    std::vector<FrameParams> frames;
+    int rc = prepare_frames(ctx, cfg, 1, frames);
+    if (rc != BH_OK) return rc;
+    const FrameParams& F = frames[0];
+    if (what == BH_EVAL_FRAME) {
+        out[0] = F.r_plus;
+        out[1] = F.r_minus;
+        out[2] = F.disc_enabled ? F.r_in : 0.0;
+        out[3] = F.disc_enabled ? F.r_out : 0.0;
+        out[4] = F.disc_enabled ? F.disc_eta : 0.0;
+        out[5] = F.disc_enabled ? F.disc_mdot : 0.0;
+        out[6] = F.r_stop;
+        out[7] = F.r_escape;
+        return BH_OK;
+    }
+    if (what == BH_EVAL_DISC_TEMPERATURE && !F.disc_enabled)
+        return fail(ctx, BH_ERR_INVALID_ARG, "the config has no disc");
+    if (n == 0) return BH_OK;
+    const size_t n_in = static_cast<size_t>(n) * (what == BH_EVAL_RHS ? 8 : 1);
+    const size_t n_out = static_cast<size_t>(n) * (what == BH_EVAL_RHS ? 8 : what == BH_EVAL_BLACKBODY ? 3 : 1);
+    if ((rc = ensure(ctx, ctx->frames, sizeof(FrameParams))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->eval_in, n_in * sizeof(double))) != BH_OK) return rc;
+    if ((rc = ensure(ctx, ctx->eval_out, n_out * sizeof(double))) != BH_OK) return rc;
+    if (what == BH_EVAL_BLACKBODY && (rc = ensure_table(ctx)) != BH_OK) return rc;
+    CK(cudaMemcpyAsync(ctx->frames.p, &F, sizeof(FrameParams), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->eval_in.p, in, n_in * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    const FrameParams* dF = static_cast<const FrameParams*>(ctx->frames.p);
+    const double* din = static_cast<const double*>(ctx->eval_in.p);
+    double* dout = static_cast<double*>(ctx->eval_out.p);
+    if (what == BH_EVAL_RHS) CK(launch_eval_rhs(cfg->precision, dF, din, n, dout, ctx->stream));
+    else CK(launch_eval_shade(what == BH_EVAL_DISC_TEMPERATURE ? 0 : 1, dF, ctx->d_table, din, n, dout, ctx->stream));
+    CK(cudaMemcpyAsync(out, dout, n_out * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BH_OK;
 }
 
 int bh_gpu_adjoint(bh_ctx* ctx, const bh_render_config* cfg, const float* target, bh_grad4* out) {

@@ -52,6 +52,7 @@ struct FrameParams {
     double pt_c[3];                  // 3 (xi-a)^2 / (xi (xi-xj)(xi-xk)), 0 where |xi| < 1e-13
     double pt_den[3];                // x0 - xi
     double disc_mdot;                // kg/s (disc.h:79)
+    double disc_eta;                 // radiative efficiency 1 - E(r_isco) (disc.h:77-78)
     double disc_rg2;                 // r_g^2 in m^2 (disc.h:96)
 
     // ---- sky ------------------------------------------------------------

@@ -76,4 +76,13 @@ struct ReduceLaunch {
 
 cudaError_t launch_reduce(const ReduceLaunch& L, cudaStream_t stream);
 
+// Known-answer evaluation of device functions (bh_gpu_eval): the trace
+// kernels' right-hand side at n states of 8 doubles (8 derivatives each),
+// and the shading's disc temperature (what 0: n radii -> n kelvin) or
+// blackbody lookup (what 1: n kelvin -> 3n XYZ).
+cudaError_t launch_eval_rhs(int precision, const FrameParams* d_frame, const double* d_in, long long n,
+                            double* d_out, cudaStream_t stream);
+cudaError_t launch_eval_shade(int what, const FrameParams* d_frame, const double* d_table, const double* d_in,
+                              long long n, double* d_out, cudaStream_t stream);
+
 }  // namespace bhg

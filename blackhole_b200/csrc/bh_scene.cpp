@@ -397,6 +397,7 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
         const double eta = 1.0 - circular_energy(ad, isco_radius(ad, sg), sg);
         const double L_edd = 4.0 * kPi * kG * c.M_kg * kMp * kC / kSigmaT;
         F.disc_mdot = c.eddington * (L_edd / (eta * kC * kC));
+        F.disc_eta = eta;
         const double r_g = kG * c.M_kg / (kC * kC);
         F.disc_rg2 = r_g * r_g;
         F.x0 = std::sqrt(F.r_in);

@@ -437,7 +437,25 @@ __global__ void reduce_final_kernel(ReduceArgs A) {
 }
 
 
+// Device shading functions at given inputs (known-answer tests): what 0,
+// the disc's effective temperature at radii in[i]; what 1, the blackbody
+// XYZ of temperatures in[i] from the device table (3 per input).
+__global__ void eval_shade_kernel(int what, const FrameParams* __restrict__ Fp, const double* __restrict__ tab,
+                                  const double* __restrict__ in, long long n, double* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (what == 0) out[i] = disc_temperature(*Fp, in[i]);
+    else blackbody(tab, in[i], out + 3 * i);
+}
+
 }  // namespace
+
+cudaError_t launch_eval_shade(int what, const FrameParams* d_frame, const double* d_table, const double* d_in,
+                              long long n, double* d_out, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    eval_shade_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(what, d_frame, d_table, d_in, n, d_out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_shade(const ShadeLaunch& L, cudaStream_t stream) {
     if (L.total_pixels <= 0) return cudaSuccess;

@@ -736,6 +736,47 @@ constexpr int kRegMixedWide = 168;
 constexpr int kRegFp64 = 168;
 constexpr int kRegFp64Wide = 232;
 
+// The right-hand side the trace kernels integrate, evaluated at given
+// states (known-answer tests of the device arithmetic): in = 8 doubles per
+// state (t, r, th, phi, p_t, p_r, p_th, p_phi), out = their derivatives
+// with respect to the affine parameter (dp_t = dp_phi = 0), with the lane
+// constants set up as start_ray sets them.
+template <class P>
+__global__ void eval_rhs_kernel(const FrameParams* __restrict__ Fp, const double* __restrict__ in, long long n,
+                                double* __restrict__ out) {
+    using R = typename P::R;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const FrameParams& F = *Fp;
+    const double* y = in + 8 * i;
+    const double E = -y[4], Lz = y[7];
+    Lane<P> L;
+    L.E = (R)E;
+    L.Lz = (R)Lz;
+    L.aR = (R)F.a;
+    L.a2R = (R)F.a2;
+    L.aE = (R)(F.a * E);
+    L.aLz = (R)(F.a * Lz);
+    L.a2E2 = (R)(F.a2 * E * E);
+    L.Lz2 = (R)(Lz * Lz);
+    L.rp_hi = (R)F.r_plus;
+    L.rp_lo = (R)(F.r_plus - (double)L.rp_hi);
+    L.rm_hi = (R)F.r_minus;
+    L.rm_lo = (R)(F.r_minus - (double)L.rm_hi);
+    L.factored = F.factored_delta;
+    R d[6];
+    rhs<P>(L, (R)y[1], (R)y[2], (R)y[5], (R)y[6], d, nullptr);
+    double* o = out + 8 * i;
+    o[0] = (double)d[0];
+    o[1] = (double)d[1];
+    o[2] = (double)d[2];
+    o[3] = (double)d[3];
+    o[4] = 0.0;
+    o[5] = (double)d[4];
+    o[6] = (double)d[5];
+    o[7] = 0.0;
+}
+
 template <class P, int MAXREG, bool JET>
 cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s) {
     TraceArgs A;
@@ -788,6 +829,15 @@ cudaError_t launch_trace_t(const TraceLaunch& L, cudaStream_t stream) {
 }  // namespace
 
 size_t deferred_record_bytes() { return sizeof(Deferred); }
+
+cudaError_t launch_eval_rhs(int precision, const FrameParams* d_frame, const double* d_in, long long n,
+                            double* d_out, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((n + 127) / 128);
+    if (precision == BH_PRECISION_MIXED) eval_rhs_kernel<Mixed><<<grid, 128, 0, stream>>>(d_frame, d_in, n, d_out);
+    else eval_rhs_kernel<Fp64><<<grid, 128, 0, stream>>>(d_frame, d_in, n, d_out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
     return L.jet ? launch_trace_t<true>(L, stream) : launch_trace_t<false>(L, stream);

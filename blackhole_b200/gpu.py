@@ -75,6 +75,7 @@ def load_library():
             "bh_gpu_render_rgb": (C.c_int, [ctx_p, cfg_p, P(abi.bh_display), P(C.c_uint8), P(C.c_double), st_p]),
             "bh_gpu_render_batch_rgb": (C.c_int, [ctx_p, cfg_p, C.c_int, P(abi.bh_display), P(P(C.c_uint8)),
                                                   P(C.c_double), st_p]),
+            "bh_gpu_eval": (C.c_int, [ctx_p, cfg_p, C.c_int, P(C.c_double), C.c_longlong, P(C.c_double)]),
             "bh_gpu_adjoint": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4)]),
             "bh_gpu_adjoint_rays": (C.c_int, [ctx_p, cfg_p, P(C.c_float), P(abi.bh_grad4), P(C.c_double),
                                               P(C.c_double)]),
@@ -256,6 +257,34 @@ class Renderer:
         return outs, list(ex)
 
     # -- discrete adjoint ----------------------------------------------------------
+    def eval(self, cfg, what: int, inputs=None):
+        """The render path's device functions at given inputs (bh_gpu_eval):
+        abi.EVAL_RHS (states (n, 8) -> derivatives (n, 8), in cfg's
+        precision), EVAL_DISC_TEMPERATURE (radii (n,) -> kelvin (n,)),
+        EVAL_BLACKBODY (kelvin (n,) -> XYZ (n, 3)), EVAL_FRAME (-> the 8 frame
+        constants r_+, r_-, r_in, r_out, efficiency, accretion rate, stop and
+        escape radius)."""
+        c = _as_c(cfg)
+        dp = C.POINTER(C.c_double)
+        if what == abi.EVAL_FRAME:
+            out = np.zeros(8)
+            self._check(self.lib.bh_gpu_eval(self._h, C.byref(c), what, None, 1, out.ctypes.data_as(dp)))
+            return out
+        x = np.ascontiguousarray(inputs, dtype=np.float64)
+        if what == abi.EVAL_RHS:
+            x = x.reshape(-1, 8)
+            shape = x.shape
+        elif what == abi.EVAL_BLACKBODY:
+            x = x.reshape(-1)
+            shape = (x.shape[0], 3)
+        else:
+            x = x.reshape(-1)
+            shape = x.shape
+        out = np.zeros(shape)
+        self._check(self.lib.bh_gpu_eval(self._h, C.byref(c), what, x.ctypes.data_as(dp), x.shape[0],
+                                         out.ctypes.data_as(dp)))
+        return out
+
     def adjoint(self, cfg, target, per_ray: bool = False):
         """Loss sum((Y - target)^2) over the pixels of the binary64 frame of
         `cfg` (Y = CIE Y, W m^-2 sr^-1) and its gradient with respect to

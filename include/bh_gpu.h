@@ -456,6 +456,26 @@ int  bh_gpu_render_rgb(bh_ctx* ctx, const bh_render_config* cfg, const bh_displa
 int  bh_gpu_render_batch_rgb(bh_ctx* ctx, const bh_render_config* cfgs, int n, const bh_display* d,
                              uint8_t* const* outs_rgb, double* exposure_used, bh_render_stats* stats);
 
+/* What bh_gpu_eval evaluates. */
+enum {
+    BH_EVAL_RHS = 0,              /* in: n states of 8 doubles (t, r, th, phi, p_t, p_r, p_th, p_phi);
+                                     out: n x 8 derivatives d/d lambda (the trace kernels' right-hand
+                                     side in cfg->precision; dp_t = dp_phi = 0) */
+    BH_EVAL_DISC_TEMPERATURE = 1, /* in: n radii (M); out: n Novikov-Thorne effective temperatures (K)
+                                     of cfg's disc, as the shading evaluates them */
+    BH_EVAL_BLACKBODY = 2,        /* in: n temperatures (K); out: n x 3 CIE XYZ (W m^-2 sr^-1) from the
+                                     device's blackbody table */
+    BH_EVAL_FRAME = 3             /* in: unused (n = 1); out: 8 frame constants of cfg: r_+, r_-, r_in
+                                     (the ISCO), r_out, the efficiency 1 - E_isco, the accretion rate
+                                     (kg/s), the stop radius, the escape radius */
+};
+
+/* The device functions of the render path evaluated at caller-given inputs
+   (host buffers), for known-answer tests of the GPU arithmetic against
+   closed forms and the reference's own checks (validate.cpp sections 1, 3,
+   6, 7).  Synchronous.  No counterpart in the reference. */
+int  bh_gpu_eval(bh_ctx* ctx, const bh_render_config* cfg, int what, const double* in, long long n, double* out);
+
 /* Measured FMA throughput of `device` in TFLOP/s (2 FLOP per FMA) for
    BH_PRECISION_FP64 (binary64) or BH_PRECISION_MIXED (binary32): the ALU
    roofline of the trace kernel.  Extension; no counterpart in the reference. */
