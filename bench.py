@@ -39,7 +39,9 @@ METRIC = "rays/s at 1024² on 1 B200: mixed vs FP64 plain at stated g/dir error;
 WORKLOAD = ("edge_on_1024: a=0.998, inclination 85 deg, 1024x1024, 1 spp, +-25 M from r=1000 M, "
             "disc r_isco..50 M at 0.3 Eddington, M=10 M_sun, 250k-star uniform sky + 21.5 mag/arcsec^2 "
             "background, escape 1.1 r_obs, horizon stop r_+(1+1e-6), rtol 1e-8 / atol 1e-10 (FP64), "
-            "1e-6 / 1e-8 (mixed)")
+            "1e-6 / 1e-8 (mixed); FP64 under the reference's step cap, mixed with error-controlled steps "
+            "(no cap: no Sun, neutron star or jet in view) and ingoing rays inside the innermost photon "
+            "orbit ended as captured")
 L2_FLUSH_BYTES = 256 << 20
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "trace_kernel_traffic.txt")
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -372,11 +374,12 @@ def animation_leg(r, frames=48, width=512, height=288):
     """A hot-spot film made the CLI's way: exposure metered on a probe of the
     middle frame, then all frames traced in one launch and developed on the
     device (bh_gpu_render_batch_rgb); wall clock from the configs to the
-    8-bit frames in host memory."""
+    8-bit frames in host memory, after one warm-up pass of the same film."""
     from blackhole_b200 import workloads
 
     film = workloads.hotspot_orbit(frames=frames, width=width, height=height)
-    r.render_batch_rgb(film[:2], exposure=1.0)             # warm-up
+    # warm-up: the same film once (buffers sized, the batch graph captured)
+    r.render_batch_rgb(film, exposure=1.0)
     t0 = time.perf_counter()
     _, e = r.render_rgb(workloads.exposure_probe(film[len(film) // 2]), meter_only=True)
     _, used = r.render_batch_rgb(film, exposure=e)
@@ -525,6 +528,22 @@ def gpu_arm(args):
                        "steps_per_ray": round(st_d.steps / st_d.rays, 2),
                        "attempts_per_ray": round(st_d.attempts / st_d.rays, 2)}
         out["mixed_over_fp64"] = round(value / v64, 3)
+
+        # The mixed path under the reference's step cap and with every
+        # captured ray traced to the stop radius: the same step sequence
+        # rule as the FP64 path, for comparison.
+        cfg_c = frame_config(size, rank, world, abi.PRECISION_MIXED)
+        cfg_c.mixed_step_limit = abi.STEP_LIMIT_REFERENCE
+        cfg_c.mixed_capture = abi.CAPTURE_REFERENCE
+        t_c, _, st_c, _ = time_device(r, cfg_c, max(2, args.steps // 2), 1, torch, flush, barrier)
+        t_c = max_over_ranks(t_c)
+        out["mixed_reference_cap"] = {
+            "value": round(world * rays * max(2, args.steps // 2) / (t_c * 1e-3), 1), "unit": "rays/s",
+            "ms_per_step": round(t_c / max(2, args.steps // 2), 4),
+            "steps_per_ray": round(st_c.steps / st_c.rays, 2),
+            "attempts_per_ray": round(st_c.attempts / st_c.rays, 2),
+            "roofline_frac": roofline(st_c.kernel_ms, st_c.steps, st_c.attempts, "mixed",
+                                      gpu.fma_peak_tflops(local, abi.PRECISION_MIXED), "")["frac"]}
 
     out["steps_per_ray"] = round(st_m.steps / st_m.rays, 2)
     out["attempts_per_ray"] = round(st_m.attempts / st_m.rays, 2)

@@ -36,6 +36,8 @@ HIT_HORIZON, HIT_DISC, HIT_SUN, HIT_STAR, HIT_SKY, HIT_EXHAUSTED = range(6)
 # Display tone curves, in img::ToneMap order (image.h:16).
 TONEMAP_LINEAR, TONEMAP_REINHARD, TONEMAP_ACES, TONEMAP_LOG, TONEMAP_HDR = range(5)
 EVAL_RHS, EVAL_DISC_TEMPERATURE, EVAL_BLACKBODY, EVAL_FRAME = range(4)
+STEP_LIMIT_AUTO, STEP_LIMIT_REFERENCE, STEP_LIMIT_NONE = range(3)
+CAPTURE_AUTO, CAPTURE_REFERENCE = range(2)
 TONEMAP_NAMES = ("linear", "reinhard", "aces", "log", "hdr")
 HIT_NAMES = ("Horizon", "Disc", "Sun", "Star", "Sky", "Exhausted")
 
@@ -114,6 +116,7 @@ class bh_render_config(C.Structure):
         ("stop_epsilon", C.c_double),
         ("mixed_rtol", C.c_double), ("mixed_atol", C.c_double),
         ("jet", bh_jet),
+        ("mixed_step_limit", C.c_int32), ("mixed_capture", C.c_int32),
     ]
 
 

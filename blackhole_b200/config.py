@@ -128,6 +128,11 @@ class RenderConfig:
       stop_epsilon  r_stop = r_+ (1 + stop_epsilon) under STOP_RELATIVE
       milky_way   diffuse background on/off
       mixed_rtol, mixed_atol  tolerances of the mixed path (0: rtol/atol)
+      mixed_step_limit  abi.STEP_LIMIT_* of the mixed path (AUTO: no step cap
+                  unless the Sun, a neutron star or a jet is in the scene)
+      mixed_capture  abi.CAPTURE_* of the mixed path (AUTO: a ray moving inwards
+                  inside the innermost photon orbit ends there as captured,
+                  unless a neutron star or a jet is in the scene)
     """
 
     M_kg: float = 10.0 * M_SUN
@@ -164,6 +169,8 @@ class RenderConfig:
     stop_epsilon: float = 0.0
     mixed_rtol: float = 0.0
     mixed_atol: float = 0.0
+    mixed_step_limit: int = abi.STEP_LIMIT_AUTO
+    mixed_capture: int = abi.CAPTURE_AUTO
 
     @property
     def n_rays(self) -> int:
@@ -217,6 +224,8 @@ class RenderConfig:
         c.mixed_rtol = self.mixed_rtol
         c.mixed_atol = self.mixed_atol
         c.jet = self.jet.to_c()
+        c.mixed_step_limit = self.mixed_step_limit
+        c.mixed_capture = self.mixed_capture
         return c
 
     def setup_jet(self) -> "RenderConfig":

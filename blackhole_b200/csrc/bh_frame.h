@@ -22,7 +22,10 @@ struct FrameParams {
     double r_escape;
     double rtol, atol;               // tolerances of this frame's precision
     double h0;                       // first trial step, 0.02 max(1, r_cam) (render.cpp:86)
+    double hmax_a, hmax_b;           // step cap hmax_a max(1, r - r_h) + hmax_b (render.cpp:130-131)
     double r_promote;                // innermost photon orbit: an ingoing ray below it is falling in
+    int32_t early_capture;           // mixed: end such a ray as captured there
+    int32_t pad_capture;
     int32_t max_steps;
     int32_t factored_delta;          // Delta = (r - r+)(r - r-) when a^2 < 1
 

@@ -331,6 +331,26 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     F.rtol = rtol;
     F.atol = atol;
     F.h0 = 0.02 * maxd(1.0, c.cam.r);
+    // The step cap (render.cpp:130-131).  The mixed path may drop it where no
+    // event needs it: the disc-plane and horizon tests look at step ends,
+    // which the error control keeps close together near the hole, while the
+    // Sun's probes, the neutron star's surface test and the jet's quadrature
+    // sample within each step.
+    if (c.mixed_step_limit < BH_STEP_LIMIT_AUTO || c.mixed_step_limit > BH_STEP_LIMIT_NONE) {
+        err = "unknown mixed_step_limit";
+        return BH_ERR_INVALID_ARG;
+    }
+    const bool needs_cap = c.sun_enabled || c.star.enabled || c.jet_enabled;
+    const bool capped = c.precision != BH_PRECISION_MIXED || c.mixed_step_limit == BH_STEP_LIMIT_REFERENCE ||
+                        (c.mixed_step_limit == BH_STEP_LIMIT_AUTO && needs_cap);
+    F.hmax_a = capped ? 0.05 : 1e30;
+    F.hmax_b = capped ? 0.01 : 1e30;
+    if (c.mixed_capture != BH_CAPTURE_AUTO && c.mixed_capture != BH_CAPTURE_REFERENCE) {
+        err = "unknown mixed_capture";
+        return BH_ERR_INVALID_ARG;
+    }
+    F.early_capture = (c.precision == BH_PRECISION_MIXED && c.mixed_capture == BH_CAPTURE_AUTO &&
+                       !c.star.enabled && !c.jet_enabled) ? 1 : 0;
     // Innermost (prograde equatorial) photon orbit, kerr.h:217-220 with |a|:
     // a photon from far away that is moving inwards below it has no radial
     // turning point left and falls into the hole.

@@ -384,7 +384,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     using R = typename P::R;
     const FrameParams& F = A.frames[L.frame];
     if (L.tries == 0) {
-        const double hmax = 0.05 * dmaxr(1.0, (double)L.y[1] - F.r_h) + 0.01;
+        const double hmax = F.hmax_a * dmaxr(1.0, (double)L.y[1] - F.r_h) + F.hmax_b;
         if (L.h > hmax) L.h = hmax;
     }
     if (!L.have_k1) {
@@ -622,6 +622,15 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         state8(L, ptph, yh);
     } else if (what < 0 && L.steps >= F.max_steps) {
         what = BH_HIT_EXHAUSTED;
+        state8(L, ptph, yh);
+    }
+    if (what < 0 && F.early_capture && rn < F.r_promote && k7[1] < R(0)) {
+        // Moving inwards inside the innermost photon orbit: no radial turning
+        // point is left, the ray falls into the hole, and nothing lies on
+        // its way (no neutron star, no jet; the disc is outside the ISCO).
+        // Mixed-precision frames only (early_capture is 0 for binary64 ones):
+        // here, or in the binary64 pass over the rays handed over near a pole.
+        what = BH_HIT_HORIZON;
         state8(L, ptph, yh);
     }
     if (what >= 0) {

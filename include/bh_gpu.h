@@ -81,6 +81,30 @@ enum {
     BH_STOP_RELATIVE = 1     /* r_+ (1 + stop_epsilon)                               */
 };
 
+/* The step-size limiter of the MIXED path.  The reference caps every step at
+   hmax = 0.05 max(1, r - r_+) + 0.01 (render.cpp:130-131) on top of the error
+   control; the binary64 path always does.
+     BH_STEP_LIMIT_AUTO       the reference cap when the Sun, a neutron star
+                              or a jet is in the scene (their hit tests and
+                              the jet's quadrature sample each step), steps
+                              set by the error control alone otherwise;
+     BH_STEP_LIMIT_REFERENCE  the reference cap;
+     BH_STEP_LIMIT_NONE       steps set by the error control alone. */
+enum { BH_STEP_LIMIT_AUTO = 0, BH_STEP_LIMIT_REFERENCE = 1, BH_STEP_LIMIT_NONE = 2 };
+
+/* How the MIXED path ends a ray that moves inwards inside the innermost
+   circular photon orbit.  Such a photon has no radial turning point left
+   (every turning point of a photon lies outside its spherical photon orbit,
+   and the prograde equatorial one is the innermost), so it reaches the
+   horizon; the disc lies outside the ISCO, further out still.
+     BH_CAPTURE_AUTO       ended there as captured (BH_HIT_HORIZON, with the
+                           state where it was ended) unless a neutron star or
+                           a jet is in the scene (a surface or emission on the
+                           way in); traced to the stop radius in binary64
+                           otherwise;
+     BH_CAPTURE_REFERENCE  always traced to the stop radius in binary64. */
+enum { BH_CAPTURE_AUTO = 0, BH_CAPTURE_REFERENCE = 1 };
+
 typedef struct bh_xyz {      /* spec::XYZ (spectrum.h:23-25), W m^-2 sr^-1 */
     double x, y, z;
 } bh_xyz;
@@ -173,6 +197,8 @@ typedef struct bh_render_config {
     double mixed_rtol;       /* tolerances of the MIXED path; 0 = max(rtol, 1e-6) */
     double mixed_atol;       /*                               0 = max(atol, 1e-8) */
     bh_jet jet;              /* bh::RenderConfig::jet (render.h:37)              */
+    int32_t mixed_step_limit;/* BH_STEP_LIMIT_* of the MIXED path (AUTO)           */
+    int32_t mixed_capture;   /* BH_CAPTURE_* of the MIXED path (AUTO)              */
 } bh_render_config;
 
 /* bh::RenderStats (render.h:55-69) plus extensions. */
