@@ -85,7 +85,7 @@ struct bh_ctx {
 
 namespace {
 
-constexpr int kReduceBlocks = 64;
+constexpr int kReduceBlocks = 512;
 
 int fail(bh_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;

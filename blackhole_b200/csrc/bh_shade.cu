@@ -416,24 +416,50 @@ __global__ void __launch_bounds__(kRedThreads) reduce_partial_kernel(ReduceArgs 
     }
 }
 
-__global__ void reduce_final_kernel(ReduceArgs A) {
+// One block per frame: thread t sums the partials t, t + kRedThreads, ... in
+// that order, then a fixed tree combines the threads: the same bits on every
+// run.
+__global__ void __launch_bounds__(kRedThreads) reduce_final_kernel(ReduceArgs A) {
     const int f = blockIdx.x;
-    if (threadIdx.x != 0) return;
-    FrameStats t = {};
-    double mn = 0.0, mq = 0.0;
-    for (int b = 0; b < A.bpf; ++b) {
+    __shared__ unsigned long long s_cnt[kRedThreads][10];
+    __shared__ double s_max[kRedThreads][2];
+    __shared__ double s_flux[kRedThreads];
+    unsigned long long c[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double mn = 0.0, mq = 0.0, flux = 0.0;
+    for (int b = threadIdx.x; b < A.bpf; b += kRedThreads) {
         const FrameStats& p = A.partials[(long long)f * A.bpf + b];
-        t.rays += p.rays; t.steps += p.steps; t.attempts += p.attempts;
-        t.captured += p.captured; t.disc_hits += p.disc_hits; t.sun_hits += p.sun_hits;
-        t.star_hits += p.star_hits; t.escaped += p.escaped; t.exhausted += p.exhausted;
-        t.jet_rays += p.jet_rays;
+        c[0] += p.rays; c[1] += p.steps; c[2] += p.attempts;
+        c[3] += p.captured; c[4] += p.disc_hits; c[5] += p.sun_hits;
+        c[6] += p.star_hits; c[7] += p.escaped; c[8] += p.exhausted; c[9] += p.jet_rays;
         mn = dmaxr(mn, __longlong_as_double((long long)p.max_norm_bits));
         mq = dmaxr(mq, __longlong_as_double((long long)p.max_q_bits));
-        t.total_flux += p.total_flux;
+        flux += p.total_flux;
     }
-    t.max_norm_bits = dbits(mn);
-    t.max_q_bits = dbits(mq);
-    A.out[f] = t;
+    for (int k = 0; k < 10; ++k) s_cnt[threadIdx.x][k] = c[k];
+    s_max[threadIdx.x][0] = mn;
+    s_max[threadIdx.x][1] = mq;
+    s_flux[threadIdx.x] = flux;
+    __syncthreads();
+    for (int off = kRedThreads / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) {
+            for (int k = 0; k < 10; ++k) s_cnt[threadIdx.x][k] += s_cnt[threadIdx.x + off][k];
+            s_max[threadIdx.x][0] = dmaxr(s_max[threadIdx.x][0], s_max[threadIdx.x + off][0]);
+            s_max[threadIdx.x][1] = dmaxr(s_max[threadIdx.x][1], s_max[threadIdx.x + off][1]);
+            s_flux[threadIdx.x] += s_flux[threadIdx.x + off];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        FrameStats t = {};
+        t.rays = s_cnt[0][0]; t.steps = s_cnt[0][1]; t.attempts = s_cnt[0][2];
+        t.captured = s_cnt[0][3]; t.disc_hits = s_cnt[0][4]; t.sun_hits = s_cnt[0][5];
+        t.star_hits = s_cnt[0][6]; t.escaped = s_cnt[0][7]; t.exhausted = s_cnt[0][8];
+        t.jet_rays = s_cnt[0][9];
+        t.max_norm_bits = dbits(s_max[0][0]);
+        t.max_q_bits = dbits(s_max[0][1]);
+        t.total_flux = s_flux[0];
+        A.out[f] = t;
+    }
 }
 
 
@@ -489,7 +515,7 @@ cudaError_t launch_reduce(const ReduceLaunch& L, cudaStream_t stream) {
     reduce_partial_kernel<<<dim3(L.blocks_per_frame, L.nframes), kRedThreads, 0, stream>>>(A);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    reduce_final_kernel<<<L.nframes, 32, 0, stream>>>(A);
+    reduce_final_kernel<<<L.nframes, kRedThreads, 0, stream>>>(A);
     return cudaGetLastError();
 }
 
