@@ -25,7 +25,7 @@ struct FrameParams {
     double hmax_a, hmax_b;           // step cap hmax_a max(1, r - r_h) + hmax_b (render.cpp:130-131)
     double r_promote;                // innermost photon orbit: an ingoing ray below it is falling in
     int32_t early_capture;           // mixed: end such a ray as captured there
-    int32_t pad_capture;
+    int32_t mirror_ok;               // mixed: integrate th > pi/2 as its mirror pi - th
     int32_t max_steps;
     int32_t factored_delta;          // Delta = (r - r+)(r - r-) when a^2 < 1
 

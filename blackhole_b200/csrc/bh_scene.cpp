@@ -351,6 +351,12 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     }
     F.early_capture = (c.precision == BH_PRECISION_MIXED && c.mixed_capture == BH_CAPTURE_AUTO &&
                        !c.star.enabled && !c.jet_enabled) ? 1 : 0;
+    // The mixed path integrates the southern hemisphere as its mirror image
+    // (Kerr is symmetric under th -> pi - th, p_th -> -p_th), so that a ray
+    // near either pole has a small angle, which binary32 resolves; the Sun,
+    // the neutron star's caps and the jets are not mirror-symmetric, so
+    // scenes with them keep the true angle.
+    F.mirror_ok = (c.precision == BH_PRECISION_MIXED && !c.sun_enabled && !c.star.enabled && !c.jet_enabled) ? 1 : 0;
     // Innermost (prograde equatorial) photon orbit, kerr.h:217-220 with |a|:
     // a photon from far away that is moving inwards below it has no radial
     // turning point left and falls into the hole.

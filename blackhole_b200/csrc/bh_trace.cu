@@ -139,6 +139,7 @@ struct Lane {
     double jet;              // jet emission picked up so far (jet kernels only)
     int gid, frame;
     int have_k1;
+    int mirror;              // mixed: the state holds pi - th and -p_th
     int factored;
     int bad_sc;
 };
@@ -300,6 +301,27 @@ __device__ __forceinline__ void write_hit(const TraceArgs& A, const Lane<P>& L, 
     o->attempts = L.attempts;
 }
 
+// pi in two binary32 parts: pi - th as (kPiHi - th) + kPiLo, the first
+// difference exact for pi/2 <= th <= pi.
+constexpr float kPiHi = 3.14159274f;
+constexpr float kPiLo = -8.74227766e-8f;
+
+// Reflect a binary32 lane through the equatorial plane: th -> pi - th,
+// p_th -> -p_th (and the stage and the cosine that go with them).  Kerr
+// geodesics map to Kerr geodesics under this reflection, and DP5 commutes
+// with it, so integrating the mirror image and reflecting the result back
+// gives the same ray; near the south pole the mirrored angle is small and
+// resolved to binary32's relative precision.
+template <class P>
+__device__ __forceinline__ void mirror_lane(Lane<P>& L) {
+    L.y[2] = (typename P::R)((kPiHi - (float)L.y[2]) + kPiLo);
+    L.y[5] = -L.y[5];
+    L.k1[2] = -L.k1[2];
+    L.k1[5] = -L.k1[5];
+    L.c0 = -L.c0;
+    L.mirror ^= 1;
+}
+
 // Lane set-up from an initial photon (fresh ray) or a deferred state.
 template <class P, bool JET>
 __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
@@ -370,6 +392,8 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     }
     L.errp_pow = (R)P::powd(dmaxr((double)L.err_prev, 1e-4), kBeta);
     L.inv_Q0 = (float)(1.0 / (fabs(L.Q0) + 1e-12));
+    L.mirror = 0;
+    if (P::kMixed && F.mirror_ok && !dr && (double)L.y[2] > 0.5 * kPi) mirror_lane(L);
     if (!dr && F.max_steps <= 0) {
         write_hit<P, JET>(A, L, BH_HIT_EXHAUSTED, y8);
         return false;
@@ -435,7 +459,10 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         const R e = h * (R(E1) * L.k1[i] + R(E3) * k3[i] + R(E4) * k4[i] + R(E5) * k5[i] +
                          R(E6) * k6[i] + R(E7) * k7[i]);
         if (P::kMixed) {
-            const float sc = (float)F.atol + (float)F.rtol * fmaxf(fabsf((float)L.y[i]), fabsf((float)yn[i]));
+            // the scale of the true angle where the lane holds its mirror
+            const float y0 = (i == 2 && L.mirror) ? kPiHi - (float)L.y[i] : (float)L.y[i];
+            const float y1 = (i == 2 && L.mirror) ? kPiHi - (float)yn[i] : (float)yn[i];
+            const float sc = (float)F.atol + (float)F.rtol * fmaxf(fabsf(y0), fabsf(y1));
             const float q = (float)e * Mixed::rcp(sc);
             err2f += q * q;
         } else {
@@ -634,22 +661,32 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         state8(L, ptph, yh);
     }
     if (what >= 0) {
+        if (P::kMixed && L.mirror) {          // back to the true angle
+            yh[2] = kPi - yh[2];
+            yh[6] = -yh[6];
+        }
         write_hit<P, JET>(A, L, what, yh);
         return true;
     }
     if (P::kMixed && A.deferred &&
-        ((rn < F.r_promote && k7[1] < R(0)) || ax7.sn2 < R(kPoleSin2))) {
+        ((rn < F.r_promote && k7[1] < R(0)) || (!F.mirror_ok && ax7.sn2 < R(kPoleSin2)))) {
         // Two places where binary32 state cannot carry the geodesic, handed
         // to the binary64 kernel for the rest of the ray:
         //  - moving inwards inside the innermost photon orbit: the ray is
         //    falling in, and Delta -> 0 cancels every digit of the
         //    Hamiltonian's radial terms;
         //  - within 0.01 of a pole: sin(th) carries the L_z^2 / sin^4 term,
-        //    and th = pi - 1e-5 is only resolved to 2.4e-7 in binary32.
+        //    and th = pi - 1e-5 is only resolved to 2.4e-7 in binary32 (not
+        //    where the lane integrates the mirror image: the angle from the
+        //    nearer pole is then small and resolved).
         const unsigned long long slot = atomicAdd(&A.queue->deferred, 1ull);
         Deferred* dd = &A.deferred[slot];
         #pragma unroll
         for (int i = 0; i < 6; ++i) dd->y[i] = (double)L.y[i];
+        if (L.mirror) {
+            dd->y[2] = kPi - dd->y[2];
+            dd->y[5] = -dd->y[5];
+        }
         dd->h = L.h;
         dd->Q0 = L.Q0;
         dd->err_prev = (float)L.err_prev;
@@ -663,6 +700,9 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         if (JET) A.jet[L.gid] = L.jet;   // the binary64 pass continues the sum
         return true;
     }
+    // Crossed the equatorial plane in the integrated frame: continue in the
+    // other one, so the lane's angle stays within pi/2 of the nearer pole.
+    if (P::kMixed && F.mirror_ok && L.c0 < R(0)) mirror_lane(L);
     return false;
 }
 
