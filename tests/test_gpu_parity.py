@@ -236,7 +236,15 @@ def test_autotune_keeps_results_and_picks_a_shape(renderer):
         best, ms = renderer.autotune(cfg)
         assert ms > 0 and best["block_size"] in (64, 128, 256, 512)
         assert renderer.get_launch(abi.PRECISION_MIXED) == best
-        assert np.array_equal(renderer.render(cfg), a)
+        b = renderer.render(cfg)
+        if best["reg_variant"] == old["reg_variant"]:
+            assert np.array_equal(b, a)
+        else:
+            # the other register cap is another compilation (its mul+add
+            # fusion may differ): the same frame to the parity tolerance
+            lit = a[..., 1] > 0
+            rel = np.abs(b[..., 1][lit] - a[..., 1][lit]) / a[..., 1][lit]
+            assert q(rel, 0.99) <= 10 * MIXED_G_TOL
     finally:
         renderer.set_launch(precision=abi.PRECISION_MIXED, **{k: v for k, v in old.items()})
 
