@@ -297,11 +297,17 @@ def cpu_baseline(size: int, max_seconds: float = 20.0):
         t0 = time.perf_counter()
         _, st, setup = ref.render_rows(cfg, rows, threads)
         wall = time.perf_counter() - t0 - setup
+        # the same path on one thread, over every 32nd row (a few seconds)
+        rows1 = list(range(0, cfg.height, 32))
+        _, st1, _ = ref.render_rows(cfg, rows1, 1)
         return {"value": st.rays / st.seconds, "unit": "rays/s", "cores": threads, "kind": "reference",
                 "sample": f"{len(rows)} of {cfg.height} rows ({st.rays} rays) of the {size}x{size} frame, "
                           f"reference sky and horizon stop (its only ones), trace+shade on {threads} threads, "
                           f"{st.seconds:.2f} s excluding {setup:.2f} s scene set-up",
-                "seconds": st.seconds}
+                "seconds": st.seconds,
+                "one_thread": {"value": round(st1.rays / st1.seconds, 1), "unit": "rays/s",
+                               "sample": f"{len(rows1)} rows ({st1.rays} rays), 1 thread, "
+                                         f"{st1.seconds:.2f} s"}}
     port = oracle.oracle()
     w = 64
     t0 = time.perf_counter()
