@@ -182,9 +182,16 @@ class Renderer:
         self._check(rc)
         return out
 
-    def render_batch(self, cfgs, stats: list | None = None) -> list:
+    def render_batch(self, cfgs, stats: list | None = None, outs: list | None = None) -> list:
+        """The frames of `cfgs` in one launch (bh_gpu_render_batch), into new
+        (H, W, 3) arrays or into `outs` (C-contiguous float64 arrays of those
+        shapes, e.g. pinned buffers reused from call to call)."""
         cs = (abi.bh_render_config * len(cfgs))(*[_as_c(c) for c in cfgs])
-        outs = [np.empty((c.height, c.width, 3), dtype=np.float64) for c in cs]
+        if outs is None:
+            outs = [np.empty((c.height, c.width, 3), dtype=np.float64) for c in cs]
+        elif len(outs) != len(cfgs) or any(o.shape != (c.height, c.width, 3) or o.dtype != np.float64
+                                           or not o.flags.c_contiguous for o, c in zip(outs, cs)):
+            raise ValueError("outs must hold one C-contiguous float64 (H, W, 3) array per frame")
         ptrs = (C.POINTER(abi.bh_xyz) * len(cfgs))(*[o.ctypes.data_as(C.POINTER(abi.bh_xyz)) for o in outs])
         sts = (abi.bh_render_stats * len(cfgs))()
         rc = self.lib.bh_gpu_render_batch(self._h, cs, len(cfgs), ptrs, sts)
