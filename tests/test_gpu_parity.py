@@ -290,6 +290,14 @@ def test_batch_equals_single_frames(renderer):
         assert np.array_equal(o, renderer.render(c, single))
         assert s.rays == single.rays and s.steps == single.steps
         assert s.disc_hits == single.disc_hits
+    # into caller-owned arrays, reused: the same frames, every call
+    mine = [np.full((c.height, c.width, 3), np.nan) for c in cfgs]
+    for _ in range(2):
+        got = renderer.render_batch(cfgs, outs=mine)
+        assert all(g is m for g, m in zip(got, mine))
+        assert all(np.array_equal(m, o) for m, o in zip(mine, outs))
+    with pytest.raises(ValueError):
+        renderer.render_batch(cfgs, outs=mine[:2])
 
 
 @pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
