@@ -54,16 +54,20 @@ def reduce_stats(stats: RenderStats, group=None, device=None) -> RenderStats:
     return out
 
 
-GRAD_FIELDS = ("loss", "d_spin", "d_inclination", "d_eddington", "d_r_out")
+GRAD_FIELDS = ("loss", "d_spin", "d_inclination", "d_eddington", "d_r_out",
+               "edge_spin", "edge_inclination", "held_spin", "held_inclination")
+GRAD_COUNTS = ("rays", "steps", "replayed_steps", "disc_rays", "sky_rays", "edge_candidates", "edge_cells",
+               "edge_steps", "high_order_rays")
 
 
 def reduce_grads(grad: dict, group=None, device=None) -> dict:
-    """Sum-all-reduce of one rank's adjoint result (loss and the four
-    gradients; counters summed too), on every rank."""
+    """Sum-all-reduce of one rank's adjoint result (loss, the four
+    gradients and their edge and held-out parts; counters summed too), on
+    every rank.  Fields absent from `grad` count as 0."""
     import torch
     import torch.distributed as dist
 
-    keys = GRAD_FIELDS + ("rays", "steps", "replayed_steps", "disc_rays", "sky_rays")
+    keys = GRAD_FIELDS + GRAD_COUNTS
     t = torch.tensor([float(grad.get(k, 0.0)) for k in keys], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     out = dict(grad)

@@ -50,7 +50,8 @@ def _worker(rank, world, port, q):
     frames = workloads.batch_64_frames()
     mine = shard.frames_for_rank(frames, rank, world)
     g = shard.reduce_grads({"loss": 1.0 + rank, "d_spin": [0.5, -2.0][rank], "d_inclination": 3.0,
-                            "d_eddington": 1e20 * (rank + 1), "d_r_out": 0.0, "rays": 10, "steps": 7})
+                            "d_eddington": 1e20 * (rank + 1), "d_r_out": -2.0 * (rank + 1), "rays": 10, "steps": 7,
+                            "edge_spin": 0.25, "edge_cells": 3 + rank})
     q.put((rank, tot.as_tuple() if hasattr(tot, "as_tuple") else vars(tot), mine, g))
     dist.barrier()
     dist.destroy_process_group()
@@ -71,6 +72,8 @@ def test_two_gloo_ranks_reduce_stats_and_split_frames():
     for _, tot, _, g in res:
         assert g["loss"] == 3.0 and g["d_spin"] == -1.5 and g["d_inclination"] == 6.0
         assert g["d_eddington"] == pytest.approx(3e20) and g["rays"] == 20 and g["steps"] == 14
+        assert g["d_r_out"] == -6.0 and g["edge_spin"] == 0.5 and g["edge_cells"] == 7
+        assert g["held_spin"] == 0.0 and g["edge_steps"] == 0
         assert tot["rays"] == 201 and tot["steps"] == 3000 and tot["captured"] == 1
         assert tot["disc_hits"] == 20 and tot["escaped"] == 10 and tot["attempts"] == 3003
         assert tot["max_norm_error"] == pytest.approx(2e-9)
