@@ -49,6 +49,9 @@ STRUCTS = {
     "bh_launch_params": abi.bh_launch_params,
     "bh_xyz": abi.bh_xyz,
     "bh_trace_record": abi.bh_trace_record,
+    "bh_jet": abi.bh_jet,
+    "bh_grad4": abi.bh_grad4,
+    "bh_display": abi.bh_display,
 }
 
 
@@ -112,3 +115,29 @@ def test_create_without_gpu_fails_loudly():
     with pytest.raises(gpu.BHError) as e:
         gpu.Renderer(0)
     assert e.value.code == abi.ERR_NO_DEVICE
+
+
+def test_enum_values_match_header():
+    """Every BH_* constant of the header against its Python mirror."""
+    txt = open(HEADER).read()
+    names = sorted(set(re.findall(r"\b(BH_[A-Z0-9_]+)\s*=", txt)) | set(re.findall(r"#define (BH_[A-Z0-9_]+) ", txt)))
+    lines = ['#include <stdio.h>', f'#include "{HEADER}"', "int main(void){"]
+    lines += [f'printf("{n} %d\\n", (int){n});' for n in names]
+    lines.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "enums.c")
+        exe = os.path.join(d, "enums")
+        open(src, "w").write("\n".join(lines))
+        subprocess.run(["gcc", "-std=c11", src, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    got = {k: int(v) for k, v in (line.split() for line in out.strip().splitlines())}
+    assert len(got) >= 35
+    for name, value in got.items():
+        py = name[3:]
+        if py == "GPU_ABI_VERSION":
+            py = "ABI_VERSION"
+        if hasattr(abi, py):
+            assert getattr(abi, py) == value, name
+    for py in ("OK", "ERR_INVALID_ARG", "HIT_SKY", "PRECISION_MIXED", "SKY_UNIFORM", "STOP_RELATIVE",
+               "TONEMAP_HDR", "EVAL_FRAME", "STEP_LIMIT_NONE", "CAPTURE_REFERENCE", "NOALLOC_MAX_RAYS"):
+        assert got["BH_" + py] == getattr(abi, py), py
