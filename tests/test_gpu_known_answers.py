@@ -219,3 +219,22 @@ def test_blackbody_lookup_against_the_exact_integral(renderer, orc):
     table = np.array([orc.blackbody_xyz(t) for t in T])
     assert float(np.max(np.abs(got[:, 1] - exact[:, 1]) / exact[:, 1])) < 2e-3
     assert float(np.max(np.abs(got - table) / table)) < 1e-12
+
+
+def test_eval_refuses_bad_requests(renderer):
+    import ctypes as C
+
+    from blackhole_b200.gpu import BHError
+
+    with pytest.raises(BHError) as e:
+        renderer.eval(_cfg(0.5, disc_enabled=False), abi.EVAL_DISC_TEMPERATURE, np.array([10.0]))
+    assert e.value.code == abi.ERR_INVALID_ARG
+    c = _cfg(0.5).to_c()
+    out = np.zeros(8)
+    dp = C.POINTER(C.c_double)
+    rc = renderer.lib.bh_gpu_eval(renderer.handle, C.byref(c), 7, out.ctypes.data_as(dp), 1, out.ctypes.data_as(dp))
+    assert rc == abi.ERR_INVALID_ARG
+    rc = renderer.lib.bh_gpu_eval(renderer.handle, C.byref(c), abi.EVAL_RHS, None, 4, out.ctypes.data_as(dp))
+    assert rc == abi.ERR_INVALID_ARG
+    # nothing to evaluate is no error
+    assert renderer.eval(_cfg(0.5), abi.EVAL_BLACKBODY, np.zeros(0)).shape == (0, 3)
