@@ -393,7 +393,13 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     L.errp_pow = (R)P::powd(dmaxr((double)L.err_prev, 1e-4), kBeta);
     L.inv_Q0 = (float)(1.0 / (fabs(L.Q0) + 1e-12));
     L.mirror = 0;
-    if (P::kMixed && F.mirror_ok && !dr && (double)L.y[2] > 0.5 * kPi) mirror_lane(L);
+    if (P::kMixed && F.mirror_ok && !dr && (double)L.y[2] > 0.5 * kPi) {
+        // a camera below the equator: start in the mirror image (the first
+        // attempt evaluates k1 and cos(th) there)
+        L.y[2] = (R)((kPiHi - (float)L.y[2]) + kPiLo);
+        L.y[5] = -L.y[5];
+        L.mirror = 1;
+    }
     if (!dr && F.max_steps <= 0) {
         write_hit<P, JET>(A, L, BH_HIT_EXHAUSTED, y8);
         return false;
