@@ -631,6 +631,7 @@ __host__ __device__ inline double sky_luminance(const SkyData& sky, const FrameP
                     const double4 s = sky.star_pos[k];
                     const double dot_raw = d[0] * s.x + d[1] * s.y + d[2] * s.z;
                     const double dot = dclamp(dot_raw, -1.0, 1.0);
+                    if (dot < F.cut_dot) continue;   // outside the cutoff, without the acos
                     double ang, dang2;   // angle and d(angle^2)/d(dot)
                     if (dot > 0.9999995) {
                         ang = sqrt(dmaxr(0.0, 2.0 * (1.0 - dot)));

@@ -65,6 +65,7 @@ struct FrameParams {
     int32_t pad0;
     double psf_sigma;                // 0.55 fov / width (render.cpp:413-414)
     double cutoff, inv2s2, psf_norm; // scene.h:114-118
+    double cut_dot;                  // cos(1.000001 cutoff): a star with d.s below it is outside the cutoff
     int32_t span_t;                  // scene.h:124
     int32_t pad1;
 

@@ -445,6 +445,10 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     F.sky_mode = c.sky_mode;
     F.psf_sigma = 0.55 * (c.cam.fov / c.width);
     F.cutoff = 3.0 * F.psf_sigma;
+    // Stars whose direction cosine lies below this are farther than the
+    // cutoff for certain (the margin covers the rounding of acos), so their
+    // acos need not be taken.
+    F.cut_dot = (F.cutoff * 1.000001 < kPi) ? std::cos(F.cutoff * 1.000001) : -1.0;
     F.inv2s2 = 1.0 / (2.0 * F.psf_sigma * F.psf_sigma);
     F.psf_norm = 1.0 / (2.0 * kPi * F.psf_sigma * F.psf_sigma);
     F.span_t = std::max(1, static_cast<int>(std::ceil(F.cutoff / (kPi / kLat))));

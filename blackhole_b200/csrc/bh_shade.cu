@@ -135,6 +135,7 @@ __device__ void sky_radiance(const SkyData& sky, const FrameParams& F, const dou
                 for (int k = k0; k < k1; ++k) {
                     const double4 s = sky.star_pos[k];
                     const double dot = dclamp(d[0] * s.x + d[1] * s.y + d[2] * s.z, -1.0, 1.0);
+                    if (dot < F.cut_dot) continue;   // outside the cutoff, without the acos
                     const double ang = (dot > 0.9999995) ? sqrt(dmaxr(0.0, 2.0 * (1.0 - dot))) : acos(dot);
                     if (ang > cutoff) continue;
                     const double w = norm * exp(-ang * ang * inv2s2) * s.w;
