@@ -242,8 +242,11 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
         return rc;
     if ((rc = ensure(ctx, ctx->fstats, n * sizeof(FrameStats))) != BH_OK) return rc;
     p.mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
-    bool any_jet = false;
-    for (int i = 0; i < n; ++i) any_jet = any_jet || frames[i].jet_enabled;
+    bool any_jet = false, any_sun = false;
+    for (int i = 0; i < n; ++i) {
+        any_jet = any_jet || frames[i].jet_enabled;
+        any_sun = any_sun || frames[i].sun_enabled;
+    }
     if (any_jet && (rc = ensure(ctx, ctx->jet, static_cast<size_t>(rays) * sizeof(double))) != BH_OK) return rc;
     if (p.mixed && (rc = ensure(ctx, ctx->deferred, static_cast<size_t>(rays) * deferred_record_bytes())) != BH_OK)
         return rc;
@@ -304,6 +307,7 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     }
     tl.resume_event = timed ? ctx->ev[3] : nullptr;
     tl.jet = any_jet ? static_cast<double*>(ctx->jet.p) : nullptr;
+    tl.sun = any_sun ? 1 : 0;
 
     ShadeLaunch& sl = p.sl;
     std::memset(&sl, 0, sizeof sl);

@@ -245,6 +245,58 @@ __device__ __forceinline__ void rhs_stage(const Lane<P>& L, typename P::R r, typ
     rhs_sc<P>(L, r, sn, cs, pr, pth, d, nullptr);
 }
 
+
+// ---- packed binary32 pairs ----------------------------------------------------
+// sm_100's f32x2 arithmetic: one instruction does the same binary32 operation,
+// rounded to nearest, on the two halves of a 64-bit register pair.  The stage
+// sums of the mixed kernel run on the six components as three pairs, in the
+// order and with the roundings of the scalar form (product, then fused
+// multiply-adds, then the fused y + h * sum).
+using u64 = unsigned long long;
+__device__ __forceinline__ u64 pk2(float lo, float hi) {
+    u64 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void up2(u64 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+    u64 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ u64 mul2(u64 a, u64 b) {
+    u64 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+// sum_s c[s] k_s[i] for the component pair (2j, 2j+1).
+template <int N>
+__device__ __forceinline__ u64 stage_sum_f2(int j, const float (&c)[N], const float* const (&k)[N]) {
+    u64 m = mul2(pk2(c[0], c[0]), pk2(k[0][2 * j], k[0][2 * j + 1]));
+    #pragma unroll
+    for (int s = 1; s < N; ++s) m = fma2(pk2(c[s], c[s]), pk2(k[s][2 * j], k[s][2 * j + 1]), m);
+    return m;
+}
+// out[i] = y[i] + h * sum_s c[s] k_s[i], i = 0..5.
+template <int N>
+__device__ __forceinline__ void stage_f2(const float* y, float h, const float (&c)[N],
+                                         const float* const (&k)[N], float* out) {
+    const u64 H = pk2(h, h);
+    #pragma unroll
+    for (int j = 0; j < 3; ++j)
+        up2(fma2(H, stage_sum_f2<N>(j, c, k), pk2(y[2 * j], y[2 * j + 1])), out[2 * j], out[2 * j + 1]);
+}
+// out[i] = h * sum_s c[s] k_s[i], i = 0..5 (the embedded error estimate).
+template <int N>
+__device__ __forceinline__ void scaled_sum_f2(float h, const float (&c)[N], const float* const (&k)[N],
+                                              float* out) {
+    const u64 H = pk2(h, h);
+    #pragma unroll
+    for (int j = 0; j < 3; ++j) up2(mul2(H, stage_sum_f2<N>(j, c, k)), out[2 * j], out[2 * j + 1]);
+}
+
 // Deferred ray: a mixed-precision ray handed to the binary64 kernel.
 struct Deferred {
     double y[6];
@@ -408,8 +460,10 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
 }
 
 // One step attempt.  Returns true when the lane's ray is finished here
-// (terminated, or deferred to the binary64 kernel).
-template <class P, bool JET>
+// (terminated, or deferred to the binary64 kernel).  SUN: compiled with the
+// Sun's intersection test; launches with no Sun in any frame run the kernels
+// without it (its code, taken by no lane, costs instruction-cache room).
+template <class P, bool JET, bool SUN>
 __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     using R = typename P::R;
     const FrameParams& F = A.frames[L.frame];
@@ -426,29 +480,67 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     }
     const R h = (R)L.h;
     R t[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], yn[6];
-    #pragma unroll
-    for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * R(A21) * L.k1[i];
-    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k2);
-    #pragma unroll
-    for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * (R(A31) * L.k1[i] + R(A32) * k2[i]);
-    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k3);
-    #pragma unroll
-    for (int i = 0; i < 6; ++i)
-        t[i] = L.y[i] + h * (R(A41) * L.k1[i] + R(A42) * k2[i] + R(A43) * k3[i]);
-    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k4);
-    #pragma unroll
-    for (int i = 0; i < 6; ++i)
-        t[i] = L.y[i] + h * (R(A51) * L.k1[i] + R(A52) * k2[i] + R(A53) * k3[i] + R(A54) * k4[i]);
-    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k5);
-    #pragma unroll
-    for (int i = 0; i < 6; ++i)
-        t[i] = L.y[i] + h * (R(A61) * L.k1[i] + R(A62) * k2[i] + R(A63) * k3[i] +
-                             R(A64) * k4[i] + R(A65) * k5[i]);
-    rhs_stage<P>(L, t[1], t[2], t[4], t[5], k6);
-    #pragma unroll
-    for (int i = 0; i < 6; ++i)
-        yn[i] = L.y[i] + h * (R(B1) * L.k1[i] + R(B3) * k3[i] + R(B4) * k4[i] + R(B5) * k5[i] +
-                              R(B6) * k6[i]);
+    if constexpr (P::kMixed) {
+        {
+            const float c[1] = {float(A21)};
+            const float* const k[1] = {L.k1};
+            stage_f2<1>(L.y, h, c, k, t);
+        }
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k2);
+        {
+            const float c[2] = {float(A31), float(A32)};
+            const float* const k[2] = {L.k1, k2};
+            stage_f2<2>(L.y, h, c, k, t);
+        }
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k3);
+        {
+            const float c[3] = {float(A41), float(A42), float(A43)};
+            const float* const k[3] = {L.k1, k2, k3};
+            stage_f2<3>(L.y, h, c, k, t);
+        }
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k4);
+        {
+            const float c[4] = {float(A51), float(A52), float(A53), float(A54)};
+            const float* const k[4] = {L.k1, k2, k3, k4};
+            stage_f2<4>(L.y, h, c, k, t);
+        }
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k5);
+        {
+            const float c[5] = {float(A61), float(A62), float(A63), float(A64), float(A65)};
+            const float* const k[5] = {L.k1, k2, k3, k4, k5};
+            stage_f2<5>(L.y, h, c, k, t);
+        }
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k6);
+        {
+            const float c[5] = {float(B1), float(B3), float(B4), float(B5), float(B6)};
+            const float* const k[5] = {L.k1, k3, k4, k5, k6};
+            stage_f2<5>(L.y, h, c, k, yn);
+        }
+    } else {
+        #pragma unroll
+        for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * R(A21) * L.k1[i];
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k2);
+        #pragma unroll
+        for (int i = 0; i < 6; ++i) t[i] = L.y[i] + h * (R(A31) * L.k1[i] + R(A32) * k2[i]);
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k3);
+        #pragma unroll
+        for (int i = 0; i < 6; ++i)
+            t[i] = L.y[i] + h * (R(A41) * L.k1[i] + R(A42) * k2[i] + R(A43) * k3[i]);
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k4);
+        #pragma unroll
+        for (int i = 0; i < 6; ++i)
+            t[i] = L.y[i] + h * (R(A51) * L.k1[i] + R(A52) * k2[i] + R(A53) * k3[i] + R(A54) * k4[i]);
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k5);
+        #pragma unroll
+        for (int i = 0; i < 6; ++i)
+            t[i] = L.y[i] + h * (R(A61) * L.k1[i] + R(A62) * k2[i] + R(A63) * k3[i] +
+                                 R(A64) * k4[i] + R(A65) * k5[i]);
+        rhs_stage<P>(L, t[1], t[2], t[4], t[5], k6);
+        #pragma unroll
+        for (int i = 0; i < 6; ++i)
+            yn[i] = L.y[i] + h * (R(B1) * L.k1[i] + R(B3) * k3[i] + R(B4) * k4[i] + R(B5) * k5[i] +
+                                  R(B6) * k6[i]);
+    }
     // The last stage is the next step's first (FSAL) and its angle the next
     // base angle: full sincos, so angle-addition errors never chain.
     Aux<P> ax7;
@@ -460,10 +552,17 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     // accept/reject test in binary64.
     double err2 = 0.0;
     float err2f = 0.f;
+    R ev[6];
+    if constexpr (P::kMixed) {
+        const float c[6] = {float(E1), float(E3), float(E4), float(E5), float(E6), float(E7)};
+        const float* const k[6] = {L.k1, k3, k4, k5, k6, k7};
+        scaled_sum_f2<6>(h, c, k, ev);
+    }
     #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        const R e = h * (R(E1) * L.k1[i] + R(E3) * k3[i] + R(E4) * k4[i] + R(E5) * k5[i] +
-                         R(E6) * k6[i] + R(E7) * k7[i]);
+        const R e = P::kMixed ? ev[i]
+                              : h * (R(E1) * L.k1[i] + R(E3) * k3[i] + R(E4) * k4[i] + R(E5) * k5[i] +
+                                     R(E6) * k6[i] + R(E7) * k7[i]);
         if (P::kMixed) {
             // the scale of the true angle where the lane holds its mirror
             const float y0 = (i == 2 && L.mirror) ? kPiHi - (float)L.y[i] : (float)L.y[i];
@@ -547,7 +646,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             dense_state(s_end);
         }
     }
-    if (what < 0 && F.sun_enabled) {
+    if (SUN && what < 0 && F.sun_enabled) {
         // The Sun (render.cpp:201-241): probe the dense geodesic, then bisect.
         const double a = F.a;
         auto cart = [&](double r, double th, double ph, double q[3]) {
@@ -712,7 +811,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     return false;
 }
 
-template <class P, int MAXREG, bool JET>
+template <class P, int MAXREG, bool JET, bool SUN>
 __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -770,7 +869,7 @@ __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
             continue;
         }
         if (active) {
-            if (attempt<P, JET>(A, L)) {
+            if (attempt<P, JET, SUN>(A, L)) {
                 active = false;
                 if (A.budget) atomicAdd(&A.queue->attempts, (unsigned long long)(L.attempts - L.att0));
             }
@@ -832,7 +931,7 @@ __global__ void eval_rhs_kernel(const FrameParams* __restrict__ Fp, const double
     o[7] = 0.0;
 }
 
-template <class P, int MAXREG, bool JET>
+template <class P, int MAXREG, bool JET, bool SUN>
 cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s) {
     TraceArgs A;
     A.frames = L.frames;
@@ -848,37 +947,49 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.budget = L.budget;
     A.jet = L.jet;
     A.xing = L.xing;
-    trace_kernel<P, MAXREG, JET><<<grid, block, 0, s>>>(A);
+    trace_kernel<P, MAXREG, JET, SUN><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
 }
 
-const void* kernel_of(int precision, int variant, int resume) {
-    if (precision == BH_PRECISION_MIXED && !resume)
-        return variant ? (const void*)trace_kernel<Mixed, kRegMixedWide, false>
-                       : (const void*)trace_kernel<Mixed, kRegMixed, false>;
-    return variant ? (const void*)trace_kernel<Fp64, kRegFp64Wide, false>
-                   : (const void*)trace_kernel<Fp64, kRegFp64, false>;
+// The three kernels of a precision and register cap: plain, with the Sun's
+// test, with the jet's emission (and the Sun's test).
+template <class P, int MAXREG>
+void family(const void* k[3]) {
+    k[0] = (const void*)trace_kernel<P, MAXREG, false, false>;
+    k[1] = (const void*)trace_kernel<P, MAXREG, false, true>;
+    k[2] = (const void*)trace_kernel<P, MAXREG, true, true>;
 }
 
-// The kernels of launches with a jet accumulate its emission per ray; the
-// others are compiled without that code.
-template <bool JET>
+void kernels_of(int precision, int variant, const void* k[3]) {
+    if (precision == BH_PRECISION_MIXED) {
+        if (variant) family<Mixed, kRegMixedWide>(k);
+        else family<Mixed, kRegMixed>(k);
+    } else {
+        if (variant) family<Fp64, kRegFp64Wide>(k);
+        else family<Fp64, kRegFp64>(k);
+    }
+}
+
+// The kernels of launches with a jet accumulate its emission per ray, and
+// those of launches with the Sun test for it; the others are compiled
+// without that code.
+template <bool JET, bool SUN>
 cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, int block, int variant, cudaStream_t s) {
-    return variant ? launch_t<Fp64, kRegFp64Wide, JET>(L, resume, grid, block, s)
-                   : launch_t<Fp64, kRegFp64, JET>(L, resume, grid, block, s);
+    return variant ? launch_t<Fp64, kRegFp64Wide, JET, SUN>(L, resume, grid, block, s)
+                   : launch_t<Fp64, kRegFp64, JET, SUN>(L, resume, grid, block, s);
 }
 
-template <bool JET>
+template <bool JET, bool SUN>
 cudaError_t launch_trace_t(const TraceLaunch& L, cudaStream_t stream) {
     if (L.precision == BH_PRECISION_MIXED) {
-        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide, JET>(L, 0, L.grid, L.block_size, stream)
-                                      : launch_t<Mixed, kRegMixed, JET>(L, 0, L.grid, L.block_size, stream);
+        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide, JET, SUN>(L, 0, L.grid, L.block_size, stream)
+                                      : launch_t<Mixed, kRegMixed, JET, SUN>(L, 0, L.grid, L.block_size, stream);
         if (e != cudaSuccess) return e;
         if (L.resume_event) cudaEventRecord(L.resume_event, stream);
         // The deferred rays, in binary64: every block reads the deferred count.
-        return launch_fp64<JET>(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);
+        return launch_fp64<JET, SUN>(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);
     }
-    return launch_fp64<JET>(L, 0, L.grid, L.block_size, L.reg_variant, stream);
+    return launch_fp64<JET, SUN>(L, 0, L.grid, L.block_size, L.reg_variant, stream);
 }
 
 }  // namespace
@@ -895,19 +1006,32 @@ cudaError_t launch_eval_rhs(int precision, const FrameParams* d_frame, const dou
 }
 
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
-    return L.jet ? launch_trace_t<true>(L, stream) : launch_trace_t<false>(L, stream);
+    if (L.jet) return launch_trace_t<true, true>(L, stream);
+    return L.sun ? launch_trace_t<false, true>(L, stream) : launch_trace_t<false, false>(L, stream);
 }
 
 int trace_blocks_per_sm(int precision, int block_size, int variant) {
-    int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_of(precision, variant, 0), block_size, 0);
-    return n;
+    const void* k[3];
+    kernels_of(precision, variant, k);
+    int least = 0;
+    for (int i = 0; i < 3; ++i) {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k[i], block_size, 0);
+        if (i == 0 || n < least) least = n;
+    }
+    return least;
 }
 
 int trace_registers(int precision, int variant) {
-    cudaFuncAttributes at;
-    cudaFuncGetAttributes(&at, kernel_of(precision, variant, 0));
-    return at.numRegs;
+    const void* k[3];
+    kernels_of(precision, variant, k);
+    int most = 0;
+    for (int i = 0; i < 3; ++i) {
+        cudaFuncAttributes at;
+        cudaFuncGetAttributes(&at, k[i]);
+        if (at.numRegs > most) most = at.numRegs;
+    }
+    return most;
 }
 
 }  // namespace bhg
