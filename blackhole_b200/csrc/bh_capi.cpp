@@ -242,10 +242,10 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
         return rc;
     if ((rc = ensure(ctx, ctx->fstats, n * sizeof(FrameStats))) != BH_OK) return rc;
     p.mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
-    bool any_jet = false, any_sun = false;
+    bool any_jet = false, any_surface = false;
     for (int i = 0; i < n; ++i) {
         any_jet = any_jet || frames[i].jet_enabled;
-        any_sun = any_sun || frames[i].sun_enabled;
+        any_surface = any_surface || frames[i].sun_enabled || frames[i].ns_enabled;
     }
     if (any_jet && (rc = ensure(ctx, ctx->jet, static_cast<size_t>(rays) * sizeof(double))) != BH_OK) return rc;
     if (p.mixed && (rc = ensure(ctx, ctx->deferred, static_cast<size_t>(rays) * deferred_record_bytes())) != BH_OK)
@@ -307,7 +307,7 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     }
     tl.resume_event = timed ? ctx->ev[3] : nullptr;
     tl.jet = any_jet ? static_cast<double*>(ctx->jet.p) : nullptr;
-    tl.sun = any_sun ? 1 : 0;
+    tl.surfaces = any_surface ? 1 : 0;
 
     ShadeLaunch& sl = p.sl;
     std::memset(&sl, 0, sizeof sl);

@@ -33,7 +33,7 @@ struct TraceLaunch {
                                      // frame of the launch has a jet
     double* xing;                    // radii of each ray's first two equatorial crossings
                                      // (2 per ray, zeroed before; 0 = none), or null
-    int sun;                         // 1 when a frame of the launch has the Sun
+    int surfaces;                    // 1 when a frame of the launch has the Sun or a neutron star
 };
 
 // Bytes of one deferred-ray record.
@@ -44,10 +44,10 @@ constexpr size_t kDeferredRecordBytes = 96;   // checked against the record in b
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream);
 
 // Blocks per SM that fit for a precision and block size (occupancy query;
-// the least over the plain, Sun and jet kernels of that precision and cap).
+// the least over the plain, surface and jet kernels of that precision and cap).
 int trace_blocks_per_sm(int precision, int block_size, int variant);
 // Registers per thread of the trace kernels of a precision (the most over
-// the plain, Sun and jet kernels).
+// the plain, surface and jet kernels).
 int trace_registers(int precision, int variant);
 
 struct ShadeLaunch {

@@ -135,6 +135,6 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
     const int bps64 = trace_blocks_per_sm(BH_PRECISION_FP64, 128, 0);
     tl.grid_resume = sms * (bps64 < 1 ? 1 : bps64);
     tl.resume_event = nullptr;
-    tl.sun = F.sun_enabled ? 1 : 0;
+    tl.surfaces = (F.sun_enabled || F.ns_enabled) ? 1 : 0;
     return launch_trace(tl, s) == cudaSuccess ? BH_OK : BH_ERR_CUDA;
 }

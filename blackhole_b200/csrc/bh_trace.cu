@@ -460,10 +460,11 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
 }
 
 // One step attempt.  Returns true when the lane's ray is finished here
-// (terminated, or deferred to the binary64 kernel).  SUN: compiled with the
-// Sun's intersection test; launches with no Sun in any frame run the kernels
-// without it (its code, taken by no lane, costs instruction-cache room).
-template <class P, bool JET, bool SUN>
+// (terminated, or deferred to the binary64 kernel).  SURF: compiled with the
+// Sun's and the neutron star's surface tests and the record of equatorial
+// crossings; launches that need none of them run kernels without that code
+// (taken by no lane, it still costs instruction-cache room and registers).
+template <class P, bool JET, bool SURF>
 __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     using R = typename P::R;
     const FrameParams& F = A.frames[L.frame];
@@ -617,7 +618,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     // Fraction of the step the jet integral covers: up to an occluding
     // event, all of it otherwise; < 0: none (render.cpp:107-122, 165-244).
     double s_jet = 1.0;
-    if (F.ns_enabled && rn <= F.ns_R) {
+    if (SURF && F.ns_enabled && rn <= F.ns_R) {
         // neutron-star surface (render.cpp:158-169)
         const DenseC cr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
         what = BH_HIT_STAR;
@@ -634,7 +635,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         const double s_end = dense_crossing(cth, 0.5 * kPi + m * kPi);
         const DenseC crr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
         const double rc = dense_eval(crr, s_end);
-        if (A.xing) {
+        if (SURF && A.xing) {
             // the crossings the discrete adjoint's edge pass starts from
             double* x = A.xing + 2 * L.gid;
             if (x[0] == 0.0) x[0] = rc;
@@ -646,7 +647,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             dense_state(s_end);
         }
     }
-    if (SUN && what < 0 && F.sun_enabled) {
+    if (SURF && what < 0 && F.sun_enabled) {
         // The Sun (render.cpp:201-241): probe the dense geodesic, then bisect.
         const double a = F.a;
         auto cart = [&](double r, double th, double ph, double q[3]) {
@@ -811,7 +812,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     return false;
 }
 
-template <class P, int MAXREG, bool JET, bool SUN>
+template <class P, int MAXREG, bool JET, bool SURF>
 __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -869,7 +870,7 @@ __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
             continue;
         }
         if (active) {
-            if (attempt<P, JET, SUN>(A, L)) {
+            if (attempt<P, JET, SURF>(A, L)) {
                 active = false;
                 if (A.budget) atomicAdd(&A.queue->attempts, (unsigned long long)(L.attempts - L.att0));
             }
@@ -931,7 +932,7 @@ __global__ void eval_rhs_kernel(const FrameParams* __restrict__ Fp, const double
     o[7] = 0.0;
 }
 
-template <class P, int MAXREG, bool JET, bool SUN>
+template <class P, int MAXREG, bool JET, bool SURF>
 cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s) {
     TraceArgs A;
     A.frames = L.frames;
@@ -947,12 +948,12 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.budget = L.budget;
     A.jet = L.jet;
     A.xing = L.xing;
-    trace_kernel<P, MAXREG, JET, SUN><<<grid, block, 0, s>>>(A);
+    trace_kernel<P, MAXREG, JET, SURF><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
 }
 
-// The three kernels of a precision and register cap: plain, with the Sun's
-// test, with the jet's emission (and the Sun's test).
+// The three kernels of a precision and register cap: plain, with the surface
+// tests and the crossing record, with those and the jet's emission.
 template <class P, int MAXREG>
 void family(const void* k[3]) {
     k[0] = (const void*)trace_kernel<P, MAXREG, false, false>;
@@ -971,25 +972,26 @@ void kernels_of(int precision, int variant, const void* k[3]) {
 }
 
 // The kernels of launches with a jet accumulate its emission per ray, and
-// those of launches with the Sun test for it; the others are compiled
-// without that code.
-template <bool JET, bool SUN>
+// those of launches with the Sun, a neutron star or a crossing record test
+// for the surfaces and record the crossings; the others are compiled without
+// that code.
+template <bool JET, bool SURF>
 cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, int block, int variant, cudaStream_t s) {
-    return variant ? launch_t<Fp64, kRegFp64Wide, JET, SUN>(L, resume, grid, block, s)
-                   : launch_t<Fp64, kRegFp64, JET, SUN>(L, resume, grid, block, s);
+    return variant ? launch_t<Fp64, kRegFp64Wide, JET, SURF>(L, resume, grid, block, s)
+                   : launch_t<Fp64, kRegFp64, JET, SURF>(L, resume, grid, block, s);
 }
 
-template <bool JET, bool SUN>
+template <bool JET, bool SURF>
 cudaError_t launch_trace_t(const TraceLaunch& L, cudaStream_t stream) {
     if (L.precision == BH_PRECISION_MIXED) {
-        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide, JET, SUN>(L, 0, L.grid, L.block_size, stream)
-                                      : launch_t<Mixed, kRegMixed, JET, SUN>(L, 0, L.grid, L.block_size, stream);
+        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide, JET, SURF>(L, 0, L.grid, L.block_size, stream)
+                                      : launch_t<Mixed, kRegMixed, JET, SURF>(L, 0, L.grid, L.block_size, stream);
         if (e != cudaSuccess) return e;
         if (L.resume_event) cudaEventRecord(L.resume_event, stream);
         // The deferred rays, in binary64: every block reads the deferred count.
-        return launch_fp64<JET, SUN>(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);
+        return launch_fp64<JET, SURF>(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);
     }
-    return launch_fp64<JET, SUN>(L, 0, L.grid, L.block_size, L.reg_variant, stream);
+    return launch_fp64<JET, SURF>(L, 0, L.grid, L.block_size, L.reg_variant, stream);
 }
 
 }  // namespace
@@ -1007,7 +1009,7 @@ cudaError_t launch_eval_rhs(int precision, const FrameParams* d_frame, const dou
 
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
     if (L.jet) return launch_trace_t<true, true>(L, stream);
-    return L.sun ? launch_trace_t<false, true>(L, stream) : launch_trace_t<false, false>(L, stream);
+    return (L.surfaces || L.xing) ? launch_trace_t<false, true>(L, stream) : launch_trace_t<false, false>(L, stream);
 }
 
 int trace_blocks_per_sm(int precision, int block_size, int variant) {
