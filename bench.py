@@ -220,8 +220,21 @@ def hbm_side(traffic, kernel_ms):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
 
 
+# Conditioning probe of a sky ray's final direction: the FP64 frame again with
+# the camera turned by COND_YAW.  At r = 1000 M that turn moves each ray's
+# image-plane impact parameter by 1.5e-7 M, the size of the change binary32
+# rounding makes to a ray's constants of motion (E, L_z, p_th at ~3e-8
+# relative).  A ray whose FP64 direction moves by more than COND_LIMIT under it
+# cannot be resolved to 1e-4 rad from any binary32 state.
+COND_YAW = 1.5e-10
+COND_LIMIT = 1e-5
+
+
 def accuracy(r, size, rank, world, cfgs=None):
-    """Per-ray error of the mixed frame against the FP64 frame (same rays)."""
+    """Per-ray error of the mixed frame against the FP64 frame (same rays),
+    with the conditioning probe of the sky rays."""
+    import copy
+
     from blackhole_b200 import abi
 
     if cfgs is None:
@@ -229,10 +242,12 @@ def accuracy(r, size, rank, world, cfgs=None):
                 frame_config(size, rank, world, abi.PRECISION_MIXED))
     a = r.trace_rays(cfgs[0])
     b = r.trace_rays(cfgs[1])
-    return compare_rays(a, b)
+    turned = copy.deepcopy(cfgs[0])
+    turned.cam.yaw += COND_YAW
+    return compare_rays(a, b, probe=r.trace_rays(turned))
 
 
-def compare_rays(a, b):
+def compare_rays(a, b, probe=None):
     from blackhole_b200 import abi
 
     same = a["what"] == b["what"]
@@ -247,6 +262,22 @@ def compare_rays(a, b):
         d = 2 * np.arcsin(np.clip(np.linalg.norm(b["dir"][sky] - a["dir"][sky], axis=1) / 2, 0, 1))
         out["dir_rad"] = {"p50": float(np.quantile(d, .5)), "p99": float(np.quantile(d, .99)),
                           "max": float(d.max()), "frac_le_1e-4": float((d <= 1e-4).mean()), "n": int(sky.sum())}
+        if probe is not None:
+            # kappa: how far the FP64 direction moves when the camera turns by
+            # COND_YAW (a ray that changes class under the turn counts as moved)
+            moved = np.full(int(sky.sum()), np.inf)
+            stay = probe["what"][sky] == abi.HIT_SKY
+            pd = probe["dir"][sky][stay]
+            moved[stay] = 2 * np.arcsin(np.clip(np.linalg.norm(pd - a["dir"][sky][stay], axis=1) / 2, 0, 1))
+            ill = moved > COND_LIMIT
+            well = d[~ill]
+            out["dir_rad"]["conditioning"] = {
+                "probe": "FP64 frame with the camera turned by %.1e rad" % COND_YAW,
+                "ill_conditioned_rays": int(ill.sum()),
+                "their_fp64_move_min": float(moved[ill].min()) if ill.any() else None,
+                "their_error_max": float(d[ill].max()) if ill.any() else None,
+                "max_well_conditioned": float(well.max()) if well.size else None,
+                "frac_le_1e-4_well_conditioned": float((well <= 1e-4).mean()) if well.size else None}
     return out
 
 

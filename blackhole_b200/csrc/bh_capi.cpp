@@ -41,8 +41,9 @@ struct bh_ctx {
     cudaStream_t abort_stream = nullptr;
     std::string err;
     // Launch shapes of the FP64 [0] and mixed [1] trace kernels (measured
-    // best on the 1024^2 edge-on frame: tight registers for FP64, wide for mixed).
-    bh_launch_params launch[2] = {{128, 1, 32, 0, 1}, {128, 1, 32, 0, 2}};
+    // best on the 1024^2 edge-on frame: the tight register caps, blocks of
+    // 128 for FP64 and 256 for mixed).
+    bh_launch_params launch[2] = {{128, 1, 32, 0, 1}, {256, 1, 32, 0, 1}};
     unsigned long long budget = 0;
     std::atomic<int> abort_requested{0};
     int32_t* h_one = nullptr;          // pinned 1, source of the abort copy

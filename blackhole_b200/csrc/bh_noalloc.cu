@@ -110,8 +110,8 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
     if (cudaMemcpyAsync(ray_end, &n, sizeof n, cudaMemcpyHostToDevice, s) != cudaSuccess) return BH_ERR_CUDA;
     if (n == 0) return BH_OK;
 
-    // The context API's default launch shapes: block 128, refill at 32 idle
-    // lanes, tight register cap for binary64, wide for binary32.
+    // The context API's default launch shapes: refill at 32 idle lanes, the
+    // tight register caps, blocks of 128 for binary64 and 256 for binary32.
     const bool mixed = cfg->precision == BH_PRECISION_MIXED;
     TraceLaunch tl;
     std::memset(&tl, 0, sizeof tl);
@@ -122,11 +122,11 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
     tl.hits = reinterpret_cast<HitRecord*>(d_out);
     tl.queue = queue;
     tl.precision = cfg->precision;
-    tl.block_size = 128;
+    tl.block_size = mixed ? 256 : 128;
     tl.rays_per_thread = 1;
     tl.refill = 32;
     tl.budget = 0;
-    tl.reg_variant = mixed ? 1 : 0;
+    tl.reg_variant = 0;
     const int bps = trace_blocks_per_sm(cfg->precision, tl.block_size, tl.reg_variant);
     tl.grid = sms * (bps < 1 ? 1 : bps);
     tl.deferred = mixed ? static_cast<void*>(base + kDeferredOff) : nullptr;

@@ -297,6 +297,30 @@ __device__ __forceinline__ void scaled_sum_f2(float h, const float (&c)[N], cons
     for (int j = 0; j < 3; ++j) up2(mul2(H, stage_sum_f2<N>(j, c, k)), out[2 * j], out[2 * j + 1]);
 }
 
+// One accepted step's ends and stages (k1, k3..k7) for the dense output.
+template <class R>
+struct StepData {
+    R y0[6], y1[6];
+    R k[6][6];
+};
+
+// The state at fraction s of the step on the dense polynomial
+// (geodesic.h:109-121), as the 8-component (t, r, th, phi, p_t, p_r, p_th,
+// p_phi) vector.  Not inlined: it runs once per ray, and inlined into the step
+// loop its code would take instruction-cache room from every step.
+template <class R>
+__device__ __noinline__ void dense_state_at(const StepData<R>* d, double h, double s, double pt, double pph,
+                                            double yh[8]) {
+    #pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const DenseC c = dense_coef(h, d->y0[i], d->y1[i], d->k[0][i], d->k[1][i], d->k[2][i], d->k[3][i],
+                                    d->k[4][i], d->k[5][i]);
+        yh[i < 4 ? i : i + 1] = dense_eval(c, s);
+    }
+    yh[4] = pt;
+    yh[7] = pph;
+}
+
 // Deferred ray: a mixed-precision ray handed to the binary64 kernel.
 struct Deferred {
     double y[6];
@@ -607,13 +631,21 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     int what = -1;
     double yh[8];
     auto dense_state = [&](double s_end) {
+        // Out of line (taken once per ray, at its event): the step's data go
+        // through a stack copy, so the stage arrays stay in registers.
+        StepData<R> d;
         #pragma unroll
         for (int i = 0; i < 6; ++i) {
-            const DenseC c = dense_coef(hd, L.y[i], yn[i], L.k1[i], k3[i], k4[i], k5[i], k6[i], k7[i]);
-            yh[i < 4 ? i : i + 1] = dense_eval(c, s_end);
+            d.y0[i] = L.y[i];
+            d.y1[i] = yn[i];
+            d.k[0][i] = L.k1[i];
+            d.k[1][i] = k3[i];
+            d.k[2][i] = k4[i];
+            d.k[3][i] = k5[i];
+            d.k[4][i] = k6[i];
+            d.k[5][i] = k7[i];
         }
-        yh[4] = pt;
-        yh[7] = pph;
+        dense_state_at<R>(&d, hd, s_end, pt, pph, yh);
     };
     // Fraction of the step the jet integral covers: up to an occluding
     // event, all of it otherwise; < 0: none (render.cpp:107-122, 165-244).
