@@ -604,6 +604,15 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     if (P::kMixed) err2 = (double)err2f;
     double err = sqrt(err2 / 8.0);
     if (L.bad_sc || !isfinite(err)) err = 1e10;
+    if (P::kMixed && L.Lz != R(0) && (ax7.sn < R(0)) != (L.sn0 < R(0))) {
+        // A ray with L_z != 0 never reaches the axis (Theta(th) < 0 near it:
+        // it turns at th_min ~ |L_z| / sqrt(Q + a^2 E^2)).  A binary32 step
+        // that ends across the axis has jumped over that turn, where the
+        // L_z^2 / sin^3 force changes over th_min / p_th of affine parameter
+        // and atol alone bounds the error in th: rejected, so the steps
+        // shrink until they resolve the turn.
+        err = 1e10;
+    }
     ++L.attempts;
     double fac = 0.9 * P::powd(dmaxr(err, 1e-16), -kAlpha) * (double)L.errp_pow;
     fac = dclamp(fac, 0.2, 5.0);
