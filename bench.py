@@ -40,8 +40,9 @@ WORKLOAD = ("edge_on_1024: a=0.998, inclination 85 deg, 1024x1024, 1 spp, +-25 M
             "disc r_isco..50 M at 0.3 Eddington, M=10 M_sun, 250k-star uniform sky + 21.5 mag/arcsec^2 "
             "background, escape 1.1 r_obs, horizon stop r_+(1+1e-6), rtol 1e-8 / atol 1e-10 (FP64), "
             "1e-6 / 1e-8 (mixed); FP64 under the reference's step cap, mixed with error-controlled steps "
-            "(no cap: no Sun, neutron star or jet in view) and ingoing rays inside the innermost photon "
-            "orbit ended as captured")
+            "(no cap: no Sun, neutron star or jet in view), ingoing rays inside the innermost photon "
+            "orbit ended as captured, and near-critical rays (escaping after circling close to the photon "
+            "shell) traced in binary64 by a kernel beside the binary32 one")
 L2_FLUSH_BYTES = 256 << 20
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "trace_kernel_traffic.txt")
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -587,6 +588,24 @@ def gpu_arm(args):
             "roofline_frac": roofline(st_c.kernel_ms, st_c.steps, st_c.attempts, "mixed",
                                       gpu.fma_peak_tflops(local, abi.PRECISION_MIXED), "")["frac"]}
 
+        # The mixed path with every ray in binary32 (BH_NEAR_CRITICAL_BINARY32):
+        # what tracing the near-critical rays in binary64 beside it costs, and
+        # what it buys in direction error.
+        cfg_b = frame_config(size, rank, world, abi.PRECISION_MIXED)
+        cfg_b.mixed_near_critical = abi.NEAR_CRITICAL_BINARY32
+        t_b, _, st_b, _ = time_device(r, cfg_b, max(2, args.steps // 2), 1, torch, flush, barrier)
+        t_b = max_over_ranks(t_b)
+        out["mixed_all_binary32"] = {
+            "value": round(world * rays * max(2, args.steps // 2) / (t_b * 1e-3), 1), "unit": "rays/s",
+            "ms_per_step": round(t_b / max(2, args.steps // 2), 4),
+            "steps_per_ray": round(st_b.steps / st_b.rays, 2)}
+        try:
+            acc_b = accuracy(r, size, rank, world, cfgs=(cfg_d, cfg_b))
+            out["mixed_all_binary32"]["dir_rad"] = acc_b.get("dir_rad")
+            out["mixed_all_binary32"]["g_rel_max"] = acc_b.get("g_rel", {}).get("max")
+        except Exception as e:  # noqa: BLE001 - a failed side measurement is reported, not fatal
+            out["mixed_all_binary32"]["accuracy_error"] = repr(e)
+
     out["steps_per_ray"] = round(st_m.steps / st_m.rays, 2)
     out["attempts_per_ray"] = round(st_m.attempts / st_m.rays, 2)
     out["classes"] = {"captured": st_m.captured, "disc": st_m.disc_hits, "sky": st_m.escaped,
@@ -649,9 +668,11 @@ def gpu_arm(args):
         except Exception as e:  # reported, not hidden
             out["display"] = {"error": repr(e)}
 
-    # Kernels of ours launched in the timed region per mixed step: trace,
-    # binary64 resume trace, shade, 2 reduce.
-    out["gpu_launches"] = 5 * args.steps
+    # Kernels of ours launched in the timed region per mixed step: the
+    # near-critical classification, the binary64 near-critical trace, two
+    # binary32 traces (the main grid and the blocks started after the binary64
+    # one), the binary64 resume trace, shade, 2 reduce.
+    out["gpu_launches"] = 8 * args.steps
     out["clocks"] = clk.summary()
 
     if not args.no_jets:

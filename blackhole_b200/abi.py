@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # Status codes (bh_gpu.h).
 OK = 0
@@ -38,6 +38,7 @@ TONEMAP_LINEAR, TONEMAP_REINHARD, TONEMAP_ACES, TONEMAP_LOG, TONEMAP_HDR = range
 EVAL_RHS, EVAL_DISC_TEMPERATURE, EVAL_BLACKBODY, EVAL_FRAME = range(4)
 STEP_LIMIT_AUTO, STEP_LIMIT_REFERENCE, STEP_LIMIT_NONE = range(3)
 CAPTURE_AUTO, CAPTURE_REFERENCE = range(2)
+NEAR_CRITICAL_AUTO, NEAR_CRITICAL_BINARY32 = range(2)
 TONEMAP_NAMES = ("linear", "reinhard", "aces", "log", "hdr")
 HIT_NAMES = ("Horizon", "Disc", "Sun", "Star", "Sky", "Exhausted")
 
@@ -116,7 +117,7 @@ class bh_render_config(C.Structure):
         ("stop_epsilon", C.c_double),
         ("mixed_rtol", C.c_double), ("mixed_atol", C.c_double),
         ("jet", bh_jet),
-        ("mixed_step_limit", C.c_int32), ("mixed_capture", C.c_int32),
+        ("mixed_step_limit", C.c_int32), ("mixed_capture", C.c_int32), ("mixed_near_critical", C.c_int32),
     ]
 
 

@@ -133,6 +133,9 @@ class RenderConfig:
       mixed_capture  abi.CAPTURE_* of the mixed path (AUTO: a ray moving inwards
                   inside the innermost photon orbit ends there as captured,
                   unless a neutron star or a jet is in the scene)
+      mixed_near_critical  abi.NEAR_CRITICAL_* of the mixed path (AUTO: rays
+                  that circle close to the photon shell before escaping are
+                  traced in binary64 by a kernel beside the binary32 one)
     """
 
     M_kg: float = 10.0 * M_SUN
@@ -171,6 +174,7 @@ class RenderConfig:
     mixed_atol: float = 0.0
     mixed_step_limit: int = abi.STEP_LIMIT_AUTO
     mixed_capture: int = abi.CAPTURE_AUTO
+    mixed_near_critical: int = abi.NEAR_CRITICAL_AUTO
 
     @property
     def n_rays(self) -> int:
@@ -226,6 +230,7 @@ class RenderConfig:
         c.jet = self.jet.to_c()
         c.mixed_step_limit = self.mixed_step_limit
         c.mixed_capture = self.mixed_capture
+        c.mixed_near_critical = self.mixed_near_critical
         return c
 
     def setup_jet(self) -> "RenderConfig":

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -39,6 +40,8 @@ struct bh_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t abort_stream = nullptr;
+    cudaStream_t side_stream = nullptr;     // the binary32 kernel's, beside the near-critical binary64 one
+    cudaEvent_t fork_event = nullptr, join_event = nullptr;
     std::string err;
     // Launch shapes of the FP64 [0] and mixed [1] trace kernels (measured
     // best on the 1024^2 edge-on frame: the tight register caps, blocks of
@@ -61,6 +64,7 @@ struct bh_ctx {
     HostSky sky_meta;
 
     DevBuf hits, pixels, rays, lum, frames, ray_end, pix_end, partials, fstats, deferred, jet;
+    DevBuf sel_flag, sel_list;         // near-critical classification of a mixed launch's rays
     // Adjoint: target image, per-ray gradients and luminances, checkpoint
     // slots, counters, sums and the edge pass's buffers.
     DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums, adj_xr, adj_cand, adj_edge, adj_high;
@@ -87,6 +91,12 @@ struct bh_ctx {
 namespace {
 
 constexpr int kReduceBlocks = 512;
+// Blocks of the near-critical binary64 kernel beside a mixed-precision launch.
+constexpr int kSideBlocks = 32;
+// Registers of one SM, and the registers a warp of threads using `per_thread`
+// is allocated (in units of 256).
+constexpr long long kSmRegs = 65536;
+long long warp_regs(int per_thread) { return (static_cast<long long>(per_thread) * 32 + 255) / 256 * 256; }
 
 int fail(bh_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;
@@ -209,6 +219,7 @@ void stats_add(bh_render_stats* s, const FrameStats& f) {
 // One launch of the pipeline, planned on the host.
 struct Plan {
     int n = 0;
+    int nf = 0;          // frames staged: n, or 2n with the binary64 treatment of mixed frames
     long long rays = 0, pix = 0;
     bool mixed = false;
     TraceLaunch tl;
@@ -236,25 +247,32 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     int rc;
     if ((rc = ensure(ctx, ctx->hits, static_cast<size_t>(rays) * sizeof(HitRecord))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->lum, static_cast<size_t>(pix) * sizeof(double))) != BH_OK) return rc;
-    if ((rc = ensure(ctx, ctx->frames, n * sizeof(FrameParams))) != BH_OK) return rc;
+    p.mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
+    p.nf = p.mixed ? 2 * n : n;
+    if ((rc = ensure(ctx, ctx->frames, p.nf * sizeof(FrameParams))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->ray_end, n * sizeof(long long))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->pix_end, n * sizeof(long long))) != BH_OK) return rc;
     if ((rc = ensure(ctx, ctx->partials, static_cast<size_t>(n) * kReduceBlocks * sizeof(FrameStats))) != BH_OK)
         return rc;
     if ((rc = ensure(ctx, ctx->fstats, n * sizeof(FrameStats))) != BH_OK) return rc;
-    p.mixed = frames[0].precision_tag == BH_PRECISION_MIXED;
-    bool any_jet = false, any_surface = false;
+    bool any_jet = false, any_surface = false, any_near_critical = false;
     for (int i = 0; i < n; ++i) {
         any_jet = any_jet || frames[i].jet_enabled;
+        any_near_critical = any_near_critical || frames[i].fp64_near_critical;
         any_surface = any_surface || frames[i].sun_enabled || frames[i].ns_enabled;
     }
     if (any_jet && (rc = ensure(ctx, ctx->jet, static_cast<size_t>(rays) * sizeof(double))) != BH_OK) return rc;
     if (p.mixed && (rc = ensure(ctx, ctx->deferred, static_cast<size_t>(rays) * deferred_record_bytes())) != BH_OK)
         return rc;
+    if (any_near_critical && (rc = ensure(ctx, ctx->sel_flag, static_cast<size_t>(rays))) != BH_OK) return rc;
+    if (any_near_critical && (rc = ensure(ctx, ctx->sel_list, static_cast<size_t>(rays) * sizeof(int))) != BH_OK)
+        return rc;
 
-    // Pinned staging: [frames][ray ends][pixel ends][queue state].  The
-    // previous launch's copies out of it must have completed.
-    p.stage_bytes = n * sizeof(FrameParams) + 2 * n * sizeof(long long) + sizeof(QueueState);
+    // Pinned staging: [frames][binary64 treatment of mixed frames][ray ends]
+    // [pixel ends][queue state].  The previous launch's copies out of it must
+    // have completed.
+    const size_t fbytes = static_cast<size_t>(p.nf) * sizeof(FrameParams);
+    p.stage_bytes = fbytes + 2 * n * sizeof(long long) + sizeof(QueueState);
     CK(cudaEventSynchronize(ctx->stage_free));
     if (p.stage_bytes > ctx->stage_cap) {
         if (ctx->stage) CK(cudaFreeHost(ctx->stage));
@@ -265,7 +283,11 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     }
     unsigned char* s = ctx->stage;
     std::memcpy(s, frames.data(), n * sizeof(FrameParams));
-    long long* ends = reinterpret_cast<long long*>(s + n * sizeof(FrameParams));
+    for (int i = n; i < p.nf; ++i) {
+        const FrameParams g = binary64_treatment(frames[i - n]);
+        std::memcpy(s + i * sizeof(FrameParams), &g, sizeof g);
+    }
+    long long* ends = reinterpret_cast<long long*>(s + fbytes);
     for (int i = 0; i < n; ++i) {
         ends[i] = frames[i].ray_begin + frames[i].n_rays;
         ends[n + i] = frames[i].pixel_begin + static_cast<long long>(frames[i].width) * frames[i].height;
@@ -274,7 +296,7 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     std::memset(&q, 0, sizeof q);
     q.budget = ctx->budget;
     q.abort = ctx->abort_requested.load() ? 1 : 0;
-    std::memcpy(s + n * sizeof(FrameParams) + 2 * n * sizeof(long long), &q, sizeof q);
+    std::memcpy(s + fbytes + 2 * n * sizeof(long long), &q, sizeof q);
 
     const int prec = frames[0].precision_tag;
     const bh_launch_params& lp = ctx->launch[prec == BH_PRECISION_MIXED ? 1 : 0];
@@ -309,6 +331,29 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
     tl.resume_event = timed ? ctx->ev[3] : nullptr;
     tl.jet = any_jet ? static_cast<double*>(ctx->jet.p) : nullptr;
     tl.surfaces = any_surface ? 1 : 0;
+    if (p.mixed && any_near_critical) {
+        // Near-critical rays in binary64 on kSideBlocks blocks beside the
+        // binary32 kernel.  The binary32 grid gives up the slots those blocks
+        // take, so that both are resident at once whichever is placed first;
+        // as many binary32 blocks start in those slots after them.
+        tl.near_critical = 1;
+        tl.grid_side = std::min(kSideBlocks, ctx->sm_count);
+        tl.frames_side = static_cast<const FrameParams*>(ctx->frames.p) + n;
+        tl.side_stream = ctx->side_stream;
+        tl.fork_event = ctx->fork_event;
+        tl.join_event = ctx->join_event;
+        tl.sel_flag = static_cast<unsigned char*>(ctx->sel_flag.p);
+        tl.sel_list = static_cast<int*>(ctx->sel_list.p);
+        tl.grid_list = ctx->sm_count * std::max(1, trace_blocks_per_sm(BH_PRECISION_FP64, 128, 0));
+        if (lp.blocks_per_sm <= 0) {
+            const long long side_regs = 4 * warp_regs(trace_registers(BH_PRECISION_FP64, 0));
+            const long long block_regs = (lp.block_size / 32) * warp_regs(trace_registers(prec, tl.reg_variant));
+            const int beside = block_regs > 0 ? static_cast<int>((kSmRegs - side_regs) / block_regs) : bps;
+            const int lost = std::max(0, bps - std::max(0, beside));
+            tl.grid_late = std::min(tl.grid - 1, tl.grid_side * lost);
+            tl.grid -= tl.grid_late;
+        }
+    }
 
     ShadeLaunch& sl = p.sl;
     std::memset(&sl, 0, sizeof sl);
@@ -344,13 +389,13 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
 int record_launch(bh_ctx* ctx, const Plan& p, cudaStream_t stream, bool timed, bool captured = false) {
     const int n = p.n;
     const unsigned char* s = ctx->stage;
-    CK(cudaMemcpyAsync(ctx->frames.p, s, n * sizeof(FrameParams), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(ctx->ray_end.p, s + n * sizeof(FrameParams), n * sizeof(long long),
+    const size_t fbytes = static_cast<size_t>(p.nf) * sizeof(FrameParams);
+    CK(cudaMemcpyAsync(ctx->frames.p, s, fbytes, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->ray_end.p, s + fbytes, n * sizeof(long long), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->pix_end.p, s + fbytes + n * sizeof(long long), n * sizeof(long long),
                        cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(ctx->pix_end.p, s + n * sizeof(FrameParams) + n * sizeof(long long),
-                       n * sizeof(long long), cudaMemcpyHostToDevice, stream));
-    CK(cudaMemcpyAsync(ctx->d_queue, s + n * sizeof(FrameParams) + 2 * n * sizeof(long long),
-                       sizeof(QueueState), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->d_queue, s + fbytes + 2 * n * sizeof(long long), sizeof(QueueState),
+                       cudaMemcpyHostToDevice, stream));
     if (!captured) CK(cudaEventRecord(ctx->stage_free, stream));
     if (timed) CK(cudaEventRecord(ctx->ev[0], stream));
     if (p.rays > 0) CK(launch_trace(p.tl, stream));
@@ -465,6 +510,9 @@ int bh_gpu_create(int device, bh_ctx** out) {
     if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
     if ((e = cudaStreamCreateWithFlags(&ctx->abort_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&ctx->fork_event, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreateWithFlags(&ctx->join_event, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
     if ((e = cudaMalloc(&ctx->d_queue, sizeof(QueueState))) != cudaSuccess) return bail(e);
     if ((e = cudaMemset(ctx->d_queue, 0, sizeof(QueueState))) != cudaSuccess) return bail(e);
     if ((e = cudaHostAlloc(&ctx->h_one, sizeof(int32_t), cudaHostAllocDefault)) != cudaSuccess) return bail(e);
@@ -484,7 +532,8 @@ void bh_gpu_destroy(bh_ctx* ctx) {
                       &ctx->pix_end, &ctx->partials, &ctx->fstats, &ctx->jet, &ctx->adj_target, &ctx->adj_grad, &ctx->adj_Y,
                       &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums, &ctx->adj_xr, &ctx->adj_cand, &ctx->adj_edge,
                       &ctx->adj_high, &ctx->eval_in, &ctx->eval_out, &ctx->disp_tmp, &ctx->disp_near,
-                      &ctx->disp_far, &ctx->disp_k, &ctx->disp_state, &ctx->disp_rgb})
+                      &ctx->disp_far, &ctx->disp_k, &ctx->disp_state, &ctx->disp_rgb, &ctx->sel_flag,
+                      &ctx->sel_list})
         if (b->p) cudaFree(b->p);
     cudaFree(ctx->d_table);
     cudaFree(ctx->d_star_pos);
@@ -499,6 +548,9 @@ void bh_gpu_destroy(bh_ctx* ctx) {
         if (ev) cudaEventDestroy(ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->abort_stream) cudaStreamDestroy(ctx->abort_stream);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    if (ctx->fork_event) cudaEventDestroy(ctx->fork_event);
+    if (ctx->join_event) cudaEventDestroy(ctx->join_event);
     delete ctx;
 }
 

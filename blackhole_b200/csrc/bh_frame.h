@@ -23,9 +23,11 @@ struct FrameParams {
     double rtol, atol;               // tolerances of this frame's precision
     double h0;                       // first trial step, 0.02 max(1, r_cam) (render.cpp:86)
     double hmax_a, hmax_b;           // step cap hmax_a max(1, r - r_h) + hmax_b (render.cpp:130-131)
+    double rtol_ref, atol_ref;       // the binary64 path's tolerances (the config's rtol, atol)
     double r_promote;                // innermost photon orbit: an ingoing ray below it is falling in
     int32_t early_capture;           // mixed: end such a ray as captured there
     int32_t mirror_ok;               // mixed: integrate th > pi/2 as its mirror pi - th
+    int32_t fp64_near_critical;      // mixed: near-critical rays traced in binary64
     int32_t max_steps;
     int32_t factored_delta;          // Delta = (r - r+)(r - r-) when a^2 < 1
 
@@ -131,6 +133,9 @@ struct QueueState {
     unsigned long long budget;       // 0 = none
     unsigned long long deferred;     // rays handed from binary32 to binary64
     unsigned long long resume_next;  // next unclaimed deferred ray
+    unsigned long long select_next;  // next near-critical ray the binary64 kernel takes (list or scan)
+    unsigned long long selected;     // near-critical rays the classification pass listed
+    unsigned long long select_next2; // next listed ray of the binary64 pass after the binary32 kernels
     int32_t abort;                   // set by the host (1) or by the budget check (2)
     int32_t status;
 };

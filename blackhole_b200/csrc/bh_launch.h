@@ -34,6 +34,22 @@ struct TraceLaunch {
     double* xing;                    // radii of each ray's first two equatorial crossings
                                      // (2 per ray, zeroed before; 0 = none), or null
     int surfaces;                    // 1 when a frame of the launch has the Sun or a neutron star
+    // Mixed precision: near-critical rays (escaping rays that circle close to
+    // the photon shell) traced by a binary64 kernel of grid_side blocks of 128
+    // on `stream`, beside the binary32 kernel on side_stream (fork_event /
+    // join_event order it against `stream`), or before it on `stream` when
+    // side_stream is null.
+    int near_critical;
+    int grid_side;
+    int grid_late;                   // binary32 blocks started on `stream` after the binary64 kernel
+    int grid_list;                   // blocks of 128 of the binary64 pass over the listed rays left
+                                     // after the binary32 kernels (beyond grid_side * 128 of them)
+    const FrameParams* frames_side;  // device: the frames under binary64_treatment
+    unsigned char* sel_flag;         // device, total_rays: near-critical flags (classification
+                                     // pass), or null: then both kernels test each ray themselves
+    int* sel_list;                   // device, total_rays: the near-critical rays' ids
+    cudaStream_t side_stream;
+    cudaEvent_t fork_event, join_event;
 };
 
 // Bytes of one deferred-ray record.

@@ -35,7 +35,8 @@ namespace {
 constexpr size_t kQueueOff = 0;
 constexpr size_t kFrameOff = 256;
 constexpr size_t kFrameBytes = (sizeof(FrameParams) + 255) / 256 * 256;
-constexpr size_t kRayEndOff = kFrameOff + kFrameBytes;
+constexpr size_t kFrameSideOff = kFrameOff + kFrameBytes;   // the frame under binary64_treatment
+constexpr size_t kRayEndOff = kFrameSideOff + kFrameBytes;
 constexpr size_t kDeferredOff = kRayEndOff + 256;
 constexpr size_t kScratchBytes = kDeferredOff + (size_t)BH_NOALLOC_MAX_RAYS * kDeferredRecordBytes;
 
@@ -107,6 +108,9 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
     // Counters start at zero on every call; the array keeps the last call's.
     if (cudaMemsetAsync(queue, 0, sizeof(QueueState), s) != cudaSuccess) return BH_ERR_CUDA;
     if (cudaMemcpyAsync(frame, &F, sizeof F, cudaMemcpyHostToDevice, s) != cudaSuccess) return BH_ERR_CUDA;
+    FrameParams* frame_side = reinterpret_cast<FrameParams*>(base + kFrameSideOff);
+    const FrameParams G = binary64_treatment(F);
+    if (cudaMemcpyAsync(frame_side, &G, sizeof G, cudaMemcpyHostToDevice, s) != cudaSuccess) return BH_ERR_CUDA;
     if (cudaMemcpyAsync(ray_end, &n, sizeof n, cudaMemcpyHostToDevice, s) != cudaSuccess) return BH_ERR_CUDA;
     if (n == 0) return BH_OK;
 
@@ -136,5 +140,11 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
     tl.grid_resume = sms * (bps64 < 1 ? 1 : bps64);
     tl.resume_event = nullptr;
     tl.surfaces = (F.sun_enabled || F.ns_enabled) ? 1 : 0;
+    // Near-critical rays in binary64 as the context API traces them, here
+    // before the binary32 kernel on the caller's stream (no stream of our own).
+    tl.near_critical = F.fp64_near_critical;
+    tl.grid_side = sms;
+    tl.frames_side = frame_side;
+    tl.side_stream = nullptr;
     return launch_trace(tl, s) == cudaSuccess ? BH_OK : BH_ERR_CUDA;
 }

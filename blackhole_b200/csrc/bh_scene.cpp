@@ -27,6 +27,9 @@ constexpr double kRsun = 6.957e8;
 constexpr double kTsun = 5772.0;
 constexpr double kMixedRtolFloor = 1e-6;
 constexpr double kMixedAtolFloor = 1e-8;
+// The reference's step cap hmax = kHmaxA max(1, r - r_h) + kHmaxB (render.cpp:130-131).
+constexpr double kHmaxA = 0.05;
+constexpr double kHmaxB = 0.01;
 
 double clampd(double v, double lo, double hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
 double maxd(double a, double b) { return (a < b) ? b : a; }
@@ -330,6 +333,8 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     F.r_escape = c.r_escape;
     F.rtol = rtol;
     F.atol = atol;
+    F.rtol_ref = c.rtol;
+    F.atol_ref = c.atol;
     F.h0 = 0.02 * maxd(1.0, c.cam.r);
     // The step cap (render.cpp:130-131).  The mixed path may drop it where no
     // event needs it: the disc-plane and horizon tests look at step ends,
@@ -343,8 +348,8 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     const bool needs_cap = c.sun_enabled || c.star.enabled || c.jet_enabled;
     const bool capped = c.precision != BH_PRECISION_MIXED || c.mixed_step_limit == BH_STEP_LIMIT_REFERENCE ||
                         (c.mixed_step_limit == BH_STEP_LIMIT_AUTO && needs_cap);
-    F.hmax_a = capped ? 0.05 : 1e30;
-    F.hmax_b = capped ? 0.01 : 1e30;
+    F.hmax_a = capped ? kHmaxA : 1e30;
+    F.hmax_b = capped ? kHmaxB : 1e30;
     if (c.mixed_capture != BH_CAPTURE_AUTO && c.mixed_capture != BH_CAPTURE_REFERENCE) {
         err = "unknown mixed_capture";
         return BH_ERR_INVALID_ARG;
@@ -357,6 +362,11 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     // the neutron star's caps and the jets are not mirror-symmetric, so
     // scenes with them keep the true angle.
     F.mirror_ok = (c.precision == BH_PRECISION_MIXED && !c.sun_enabled && !c.star.enabled && !c.jet_enabled) ? 1 : 0;
+    if (c.mixed_near_critical != BH_NEAR_CRITICAL_AUTO && c.mixed_near_critical != BH_NEAR_CRITICAL_BINARY32) {
+        err = "unknown mixed_near_critical";
+        return BH_ERR_INVALID_ARG;
+    }
+    F.fp64_near_critical = (c.precision == BH_PRECISION_MIXED && c.mixed_near_critical == BH_NEAR_CRITICAL_AUTO) ? 1 : 0;
     // Innermost (prograde equatorial) photon orbit, kerr.h:217-220 with |a|:
     // a photon from far away that is moving inwards below it has no radial
     // turning point left and falls into the hole.
@@ -506,6 +516,17 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
         powerlaw_xyz(j.alpha, F.jet_col);   // render.cpp:417
     }
     return BH_OK;
+}
+
+FrameParams binary64_treatment(const FrameParams& F) {
+    FrameParams G = F;
+    G.rtol = F.rtol_ref;
+    G.atol = F.atol_ref;
+    G.hmax_a = kHmaxA;
+    G.hmax_b = kHmaxB;
+    G.early_capture = 0;
+    G.mirror_ok = 0;
+    return G;
 }
 
 void jet_configure(bh_jet& j, double spin, double mdot_c2, double r_g_m) {

@@ -41,6 +41,11 @@ int star_catalogue(int count, uint64_t seed, int sky_mode, double* out6);
 // Validate a config and fill the frame constants.  Returns a bh_status.
 int make_frame(const bh_render_config& c, FrameParams& F, std::string& err);
 
+// The constants under which a mixed-precision frame's near-critical rays are
+// traced in binary64: those of the binary64 path (the config's tolerances,
+// the reference's step cap, no early capture, no mirrored hemisphere).
+FrameParams binary64_treatment(const FrameParams& F);
+
 // The reference defaults (render.h:15-53, scene.h:232-351, neutronstar.h:43-70,
 // jet.h:96-146).
 void default_config(bh_render_config& c);

@@ -345,6 +345,12 @@ struct TraceArgs {
     unsigned long long budget;
     double* jet;             // jet emission per ray (jet kernels only)
     double* xing;            // first two equatorial crossing radii per ray, or null
+    int select;              // 0: every ray; 1: near-critical rays only; 2: all others
+    const unsigned char* sel_flag;   // per ray: 1 = near-critical (classification pass), or null
+    const int* sel_list;     // the near-critical rays' global ids, or null (then select 1 scans)
+    long long list_cap;      // select 1 with a list: the rays [0, list_cap) beside the binary32
+                             // kernel (phase 0), the rest [list_cap, ..) after it (phase 1)
+    int phase;
 };
 
 template <class P>
@@ -398,6 +404,52 @@ __device__ __forceinline__ void mirror_lane(Lane<P>& L) {
     L.mirror ^= 1;
 }
 
+// Bound on |R_min| / r*^4 under which a ray is near-critical (below).
+constexpr double kNearCritical = 0.1;
+
+// Whether a photon from the camera passes close to the photon shell on its way
+// out: its radial potential per E^2 (kerr.h carter form, b = L_z/E, q = Q/E^2)
+//   R(r) = (r^2 + a^2 - a b)^2 - Delta (q + (b - a)^2)
+//        = r^4 + (a^2 - b^2 - q) r^2 + 2 (q + (b - a)^2) r - a^2 q
+// has its local minimum R_min at the largest root r* of R'; R_min < 0 is a
+// turning point (the ray escapes), and the closer R_min is to 0 the more
+// times the ray circles near r* and the more a small change of its state is
+// amplified (about e^(2 pi) per orbit).  Such rays (ingoing from outside r*,
+// -kNearCritical < R_min / r*^4 < 0) go to binary64: no binary32 state
+// resolves their final direction.  Out of line and in explicitly rounded
+// binary64, so that every kernel that calls it decides the same for a ray.
+__device__ __noinline__ bool near_critical(const FrameParams& F, const double y8[8], double Q0) {
+    if (!F.fp64_near_critical) return false;
+    // The traced photon runs backwards in time (E = -p_t < 0 for the camera's
+    // rays); b and q are the same for it as for the photon it reverses.
+    const double E = -y8[4];
+    if (!(E != 0.0) || !(y8[5] < 0.0)) return false;      // ingoing photons only
+    const double b = __ddiv_rn(y8[7], E);
+    const double q = __ddiv_rn(Q0, __dmul_rn(E, E));
+    const double bma = __dsub_rn(b, F.a);
+    const double c2 = __dsub_rn(__dsub_rn(F.a2, __dmul_rn(b, b)), q);
+    const double c1 = __dmul_rn(2.0, __dadd_rn(q, __dmul_rn(bma, bma)));
+    const double c0 = -__dmul_rn(F.a2, q);
+    if (!(c2 < 0.0)) return false;                         // R' > 0 for r > 0: no minimum
+    // Newton on R'(r) = 4 r^3 + 2 c2 r + c1 from sqrt(-c2), right of its
+    // largest root (there 2 r (2 r^2 + c2) > 0 and c1 >= 0): monotone.
+    double r = __dsqrt_rn(-c2);
+    for (int it = 0; it < 60; ++it) {
+        const double r2 = __dmul_rn(r, r);
+        const double d1 = __dadd_rn(__dmul_rn(__dmul_rn(4.0, r2), r), __dadd_rn(__dmul_rn(__dmul_rn(2.0, c2), r), c1));
+        const double d2 = __dadd_rn(__dmul_rn(12.0, r2), __dmul_rn(2.0, c2));
+        if (!(d2 > 0.0)) return false;
+        const double step = __ddiv_rn(d1, d2);
+        r = __dsub_rn(r, step);
+        if (!(fabs(step) > 1e-13 * r)) break;
+    }
+    if (!(r > F.r_plus) || !(y8[1] > r)) return false;
+    const double r2 = __dmul_rn(r, r);
+    const double R = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(__dadd_rn(r2, c2), r), c1), r), c0);
+    const double Rn = __ddiv_rn(R, __dmul_rn(r2, r2));
+    return Rn < 0.0 && Rn > -kNearCritical;
+}
+
 // Lane set-up from an initial photon (fresh ray) or a deferred state.
 template <class P, bool JET>
 __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
@@ -408,12 +460,18 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
         L.gid = dr->gid;
         L.frame = dr->frame;
     } else {
-        L.gid = (int)id;
-        L.frame = find_frame(A.frame_ray_end, A.nframes, id);
+        L.gid = (A.select == 1 && A.sel_list) ? A.sel_list[id + (A.phase ? A.list_cap : 0)] : (int)id;
+        // the binary32 kernel leaves the listed rays to the binary64 one
+        if (A.select == 2 && A.sel_flag && A.sel_flag[L.gid]) return false;
+        L.frame = find_frame(A.frame_ray_end, A.nframes, L.gid);
     }
     const FrameParams& F = A.frames[L.frame];
     double y8[8], Q0;
     ray_setup(F, (long long)L.gid - F.ray_begin, y8, &Q0);
+    // Near-critical rays of a mixed-precision launch are traced by the
+    // binary64 kernel that runs beside the binary32 one: each of the two
+    // skips the other's rays (no hit record written here).
+    if (!dr && A.select && !A.sel_flag && near_critical(F, y8, Q0) != (A.select == 1)) return false;
     const double E = -y8[4], Lz = y8[7];
     L.E = (R)E;
     L.Lz = (R)Lz;
@@ -857,9 +915,18 @@ template <class P, int MAXREG, bool JET, bool SURF>
 __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const long long total = A.resume ? (long long)*(volatile unsigned long long*)&A.queue->deferred
-                                     : A.total_rays;
-    unsigned long long* counter = A.resume ? &A.queue->resume_next : &A.queue->next;
+    long long total = A.resume ? (long long)*(volatile unsigned long long*)&A.queue->deferred : A.total_rays;
+    unsigned long long* counter = A.resume ? &A.queue->resume_next
+                                           : (A.select == 1 ? &A.queue->select_next : &A.queue->next);
+    if (!A.resume && A.select == 1 && A.sel_list) {
+        const long long listed = (long long)*(volatile unsigned long long*)&A.queue->selected;
+        if (A.phase == 0) {
+            total = listed < A.list_cap ? listed : A.list_cap;
+        } else {
+            total = listed > A.list_cap ? listed - A.list_cap : 0;
+            counter = &A.queue->select_next2;
+        }
+    }
     Lane<P> L;
     bool active = false, done = false;
     long long q_next = 0;
@@ -894,14 +961,16 @@ __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
                         q_next = (long long)base + __popc(want & lt_mask);
                         q_stride = n;
                         q_left = A.rays_per_thread;
+                        // A lane is done only when the ids run out: start_ray
+                        // also returns false for a ray it leaves to another
+                        // kernel or ends at once, and the lane then refills.
                         while (!active && q_left > 0) {
-                            if (q_next >= total) { q_left = 0; break; }
+                            if (q_next >= total) { q_left = 0; done = true; break; }
                             const long long id = q_next;
                             q_next += q_stride;
                             --q_left;
                             active = start_ray<P, JET>(A, L, id);
                         }
-                        if (!active && q_left == 0) done = true;
                     }
                 }
             }
@@ -974,9 +1043,14 @@ __global__ void eval_rhs_kernel(const FrameParams* __restrict__ Fp, const double
 }
 
 template <class P, int MAXREG, bool JET, bool SURF>
-cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s) {
+cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s, int select = 0,
+                     int phase = 0) {
     TraceArgs A;
-    A.frames = L.frames;
+    A.frames = (select == 1) ? L.frames_side : L.frames;
+    A.sel_flag = select ? L.sel_flag : nullptr;
+    A.sel_list = (select == 1) ? L.sel_list : nullptr;
+    A.list_cap = (long long)L.grid_side * 128;
+    A.phase = phase;
     A.frame_ray_end = L.frame_ray_end;
     A.nframes = L.nframes;
     A.total_rays = L.total_rays;
@@ -986,11 +1060,36 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.resume = resume;
     A.rays_per_thread = L.rays_per_thread < 1 ? 1 : L.rays_per_thread;
     A.refill = L.refill < 1 ? 1 : (L.refill > 32 ? 32 : L.refill);
+    A.select = select;
+    if (select == 1) {
+        // few rays found among many looked at: refill a lane as soon as it
+        // is idle, one id at a time, so a lane tracing a ray does not hold
+        // up the search of the other 31
+        A.rays_per_thread = 1;
+        A.refill = 1;
+    }
     A.budget = L.budget;
     A.jet = L.jet;
     A.xing = L.xing;
     trace_kernel<P, MAXREG, JET, SURF><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
+}
+
+// The near-critical test of every ray's initial photon (grid-stride, one
+// thread per ray): flag[id] = 1 and the id appended to `list` for the rays
+// the binary64 kernel beside the binary32 one traces.
+__global__ void classify_kernel(const FrameParams* __restrict__ frames, const long long* __restrict__ frame_ray_end,
+                                int nframes, long long total, QueueState* queue, unsigned char* __restrict__ flag,
+                                int* __restrict__ list) {
+    for (long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x; id < total;
+         id += (long long)gridDim.x * blockDim.x) {
+        const FrameParams& F = frames[find_frame(frame_ray_end, nframes, id)];
+        double y8[8], Q0;
+        ray_setup(F, id - F.ray_begin, y8, &Q0);
+        const bool nc = near_critical(F, y8, Q0);
+        flag[id] = nc ? 1 : 0;
+        if (nc) list[atomicAdd(&queue->selected, 1ull)] = (int)id;
+    }
 }
 
 // The three kernels of a precision and register cap: plain, with the surface
@@ -1025,9 +1124,54 @@ cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, int block, i
 template <bool JET, bool SURF>
 cudaError_t launch_trace_t(const TraceLaunch& L, cudaStream_t stream) {
     if (L.precision == BH_PRECISION_MIXED) {
-        cudaError_t e = L.reg_variant ? launch_t<Mixed, kRegMixedWide, JET, SURF>(L, 0, L.grid, L.block_size, stream)
-                                      : launch_t<Mixed, kRegMixed, JET, SURF>(L, 0, L.grid, L.block_size, stream);
-        if (e != cudaSuccess) return e;
+        cudaError_t e;
+        const bool side = L.near_critical && L.side_stream && L.fork_event && L.join_event;
+        if (L.near_critical) {
+            // The near-critical rays in binary64 (the kernel of the binary64
+            // path's default cap, blocks of 128: the same arithmetic as a
+            // binary64 frame) beside the binary32 launch (the two
+            // share no data but the queue's separate counters and never wait
+            // on each other), or before it on the same stream.  With a flag
+            // array, a classification pass lists them first.
+            if (L.sel_flag) {
+                const long long want = (L.total_rays + 255) / 256;
+                const int cgrid = (int)(want < 4LL * L.grid ? want : 4LL * L.grid);
+                classify_kernel<<<cgrid > 0 ? cgrid : 1, 256, 0, stream>>>(L.frames, L.frame_ray_end, L.nframes,
+                                                                          L.total_rays, L.queue, L.sel_flag,
+                                                                          L.sel_list);
+                if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            }
+        }
+        // Beside: the binary32 kernel on the side stream from the fork on, with
+        // the block slots the binary64 kernel's blocks leave; on `stream` the
+        // binary64 kernel, then binary32 blocks for those slots, which take
+        // from the same queue whatever is left when the binary64 blocks are
+        // done (neither kernel waits for the other).  The pass over rays the
+        // binary32 kernels hand over runs after both, on `stream`.
+        const int sel = L.near_critical ? 2 : 0;
+        auto launch32 = [&](int grid, cudaStream_t s) {
+            return L.reg_variant ? launch_t<Mixed, kRegMixedWide, JET, SURF>(L, 0, grid, L.block_size, s, sel)
+                                 : launch_t<Mixed, kRegMixed, JET, SURF>(L, 0, grid, L.block_size, s, sel);
+        };
+        if (side) {
+            if ((e = cudaEventRecord(L.fork_event, stream)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(L.side_stream, L.fork_event, 0)) != cudaSuccess) return e;
+        }
+        if (L.near_critical &&
+            (e = launch_t<Fp64, kRegFp64, JET, SURF>(L, 0, L.grid_side, 128, stream, 1)) != cudaSuccess)
+            return e;
+        if ((e = launch32(L.grid, side ? L.side_stream : stream)) != cudaSuccess) return e;
+        if (side) {
+            if (L.grid_late > 0 && (e = launch32(L.grid_late, stream)) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(L.join_event, L.side_stream)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(stream, L.join_event, 0)) != cudaSuccess) return e;
+        }
+        // Listed near-critical rays beyond one per lane of the binary64 kernel
+        // beside (a frame dense in them, like one centred on the photon ring):
+        // on the whole GPU once the binary32 kernels are done.
+        if (L.near_critical && L.sel_list &&
+            (e = launch_t<Fp64, kRegFp64, JET, SURF>(L, 0, L.grid_list, 128, stream, 1, 1)) != cudaSuccess)
+            return e;
         if (L.resume_event) cudaEventRecord(L.resume_event, stream);
         // The deferred rays, in binary64: every block reads the deferred count.
         return launch_fp64<JET, SURF>(L, 1, L.grid_resume, L.block_resume, L.reg_variant_resume, stream);

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define BH_GPU_ABI_VERSION 2
+#define BH_GPU_ABI_VERSION 3
 
 /* Status codes. */
 enum {
@@ -104,6 +104,19 @@ enum { BH_STEP_LIMIT_AUTO = 0, BH_STEP_LIMIT_REFERENCE = 1, BH_STEP_LIMIT_NONE =
                            otherwise;
      BH_CAPTURE_REFERENCE  always traced to the stop radius in binary64. */
 enum { BH_CAPTURE_AUTO = 0, BH_CAPTURE_REFERENCE = 1 };
+
+/* Which rays the MIXED path traces in binary64 from the start.  A photon whose
+   radial potential R(r) = (r^2 + a^2 - a b)^2 - Delta (q + (b - a)^2) (b = L_z/E,
+   q = Q/E^2) dips to just below zero at its minimum r* escapes after circling
+   close to the photon shell, and every pass multiplies a change of its state
+   by ~e^(2 pi): no binary32 state resolves where it leaves to.
+     BH_NEAR_CRITICAL_AUTO      ingoing rays with -0.1 < R(r*)/r*^4 < 0 are
+                                traced in binary64 under the binary64 path's
+                                tolerances and step cap (their results are
+                                the binary64 frame's), by a kernel that runs
+                                beside the binary32 one;
+     BH_NEAR_CRITICAL_BINARY32  every ray starts in binary32. */
+enum { BH_NEAR_CRITICAL_AUTO = 0, BH_NEAR_CRITICAL_BINARY32 = 1 };
 
 typedef struct bh_xyz {      /* spec::XYZ (spectrum.h:23-25), W m^-2 sr^-1 */
     double x, y, z;
@@ -199,6 +212,7 @@ typedef struct bh_render_config {
     bh_jet jet;              /* bh::RenderConfig::jet (render.h:37)              */
     int32_t mixed_step_limit;/* BH_STEP_LIMIT_* of the MIXED path (AUTO)           */
     int32_t mixed_capture;   /* BH_CAPTURE_* of the MIXED path (AUTO)              */
+    int32_t mixed_near_critical; /* BH_NEAR_CRITICAL_* of the MIXED path (AUTO)    */
 } bh_render_config;
 
 /* bh::RenderStats (render.h:55-69) plus extensions. */

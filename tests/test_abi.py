@@ -139,5 +139,5 @@ def test_enum_values_match_header():
         if hasattr(abi, py):
             assert getattr(abi, py) == value, name
     for py in ("OK", "ERR_INVALID_ARG", "HIT_SKY", "PRECISION_MIXED", "SKY_UNIFORM", "STOP_RELATIVE",
-               "TONEMAP_HDR", "EVAL_FRAME", "STEP_LIMIT_NONE", "CAPTURE_REFERENCE", "NOALLOC_MAX_RAYS"):
+               "TONEMAP_HDR", "EVAL_FRAME", "STEP_LIMIT_NONE", "CAPTURE_REFERENCE", "NEAR_CRITICAL_BINARY32", "NOALLOC_MAX_RAYS"):
         assert got["BH_" + py] == getattr(abi, py), py

@@ -12,6 +12,10 @@ BH_STEP_LIMIT_*, BH_CAPTURE_*).
     AUTO default) changes no ray's class and no pixel: every such ray ends
     on the horizon when traced on;
   * the binary64 path ignores both knobs;
+  * near-critical rays (their radial potential's minimum just below zero:
+    they circle close to the photon shell before escaping) are the binary64
+    frame's rays bit for bit under BH_NEAR_CRITICAL_AUTO, and no other ray
+    is (BH_NEAR_CRITICAL_BINARY32 leaves all of them in binary32);
   * unknown values are refused.
 """
 import copy
@@ -112,10 +116,52 @@ def test_binary64_path_ignores_the_mixed_knobs(renderer):
 
 
 @pytest.mark.parametrize("knob,value", [("mixed_step_limit", 3), ("mixed_step_limit", -1),
-                                        ("mixed_capture", 2)])
+                                        ("mixed_capture", 2), ("mixed_near_critical", 2)])
 def test_unknown_knob_values_are_refused(renderer, knob, value):
     cfg = _edge_on(16, precision=abi.PRECISION_MIXED)
     setattr(cfg, knob, value)
     with pytest.raises(BHError) as e:
         renderer.render(cfg)
     assert e.value.code == abi.ERR_INVALID_ARG
+
+
+def _near_critical(cfg, fp64):
+    """The near-critical rule restated on the binary64 frame's constants of
+    motion (E, L_z from p_t, p_phi; Q from th, p_th at the end of the ray):
+    the minimum of R(r) / r^4 at the largest root of R' in (-0.1, 0), for rays
+    that start moving inwards from outside that root."""
+    y = fp64["y"]
+    a = cfg.spin
+    E, Lz, th, pth = -y[:, 4], y[:, 7], y[:, 2], y[:, 6]
+    b = Lz / E
+    q = (pth ** 2 + np.cos(th) ** 2 * (-(a * a) * E * E + Lz ** 2 / np.sin(th) ** 2)) / E ** 2
+    c2 = a * a - b * b - q
+    c1 = 2.0 * (q + (b - a) ** 2)
+    r = np.sqrt(np.maximum(-c2, 0.0))
+    for _ in range(60):
+        r = r - (4 * r ** 3 + 2 * c2 * r + c1) / np.where(12 * r ** 2 + 2 * c2 > 0, 12 * r ** 2 + 2 * c2, 1.0)
+    Rn = (r ** 4 + c2 * r ** 2 + c1 * r - a * a * q) / r ** 4
+    r_plus = 1.0 + np.sqrt(1.0 - a * a)
+    return (c2 < 0) & (r > r_plus) & (Rn < 0) & (Rn > -0.1)
+
+
+def test_near_critical_rays_are_the_binary64_frames(renderer):
+    cfg = _edge_on(192, precision=abi.PRECISION_FP64, stop_mode=abi.STOP_REFERENCE)
+    fp64 = renderer.trace_rays(cfg)
+    auto = renderer.trace_rays(_with(cfg, precision=abi.PRECISION_MIXED))
+    b32 = renderer.trace_rays(_with(cfg, precision=abi.PRECISION_MIXED,
+                                    mixed_near_critical=abi.NEAR_CRITICAL_BINARY32))
+    same = np.all(auto["y"] == fp64["y"], axis=1) & (auto["steps"] == fp64["steps"])
+    nc = _near_critical(cfg, fp64)     # most of them end on the disc after their orbit
+    # the restated rule reads Q at the end of the ray (conserved to ~1e-9):
+    # rays within that of the bound may fall on either side
+    assert nc.sum() >= 50, nc.sum()
+    assert same[nc].mean() >= 0.99, same[nc].mean()
+    # every ray the binary64 kernel took is near-critical (or a ray whose
+    # binary32 and binary64 integrations agree to the last bit, which a
+    # frame of this size does not have)
+    assert (same & ~nc).sum() <= 0.01 * nc.sum() + 2, (same & ~nc).sum()
+    # under BINARY32 the near-critical rays are integrated in binary32
+    assert not np.all(b32["y"][nc] == fp64["y"][nc])
+    # classes and pixels of everything else are those of BINARY32
+    assert np.array_equal(auto["what"][~nc & ~same], b32["what"][~nc & ~same])
