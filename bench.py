@@ -248,41 +248,139 @@ def accuracy(r, size, rank, world, cfgs=None):
     return compare_rays(a, b, probe=r.trace_rays(turned))
 
 
-def compare_rays(a, b, probe=None):
+def _angle(u, v):
+    """Angle between unit vectors, from the chord (stable for tiny angles)."""
+    return 2.0 * np.arcsin(np.clip(np.linalg.norm(u - v, axis=1) / 2.0, 0.0, 1.0))
+
+
+def _dist(e, tol):
+    return {"p50": float(np.quantile(e, .5)), "p99": float(np.quantile(e, .99)),
+            "p999": float(np.quantile(e, .999)), "max": float(e.max()), "n": int(e.size),
+            "n_above_target": int((e > tol).sum())}
+
+
+def conditioning(fp64, probe):
+    """How far each ray's FP64 result moves when the camera turns by COND_YAW:
+    the sky direction's angle for sky rays, |dg|/g for disc rays (inf where
+    the turn changes the class).  fp64 and probe are GPU FP64 frames of the
+    same rays, the probe with the camera turned."""
     from blackhole_b200 import abi
 
+    moved = np.full(len(fp64), np.inf)
+    sky = (fp64["what"] == abi.HIT_SKY) & (probe["what"] == abi.HIT_SKY)
+    moved[sky] = _angle(probe["dir"][sky], fp64["dir"][sky])
+    disc = (fp64["what"] == abi.HIT_DISC) & (probe["what"] == abi.HIT_DISC) & (fp64["g"] > 0)
+    moved[disc] = np.abs(probe["g"][disc] - fp64["g"][disc]) / fp64["g"][disc]
+    return moved
+
+
+def compare_rays(a, b, probe=None, moved=None, against="the FP64 GPU frame (per ray)"):
+    """Per-ray error of `b` against `a` (same rays, same order): class
+    agreement, the relative error of g over disc rays of equal class and the
+    sky-direction angle over sky rays of equal class, each with its tail
+    beyond the target (1e-3, 1e-4 rad).  `moved` (from `conditioning`) or
+    `probe` (a turned FP64 frame against `a`) marks the ill-conditioned rays,
+    whose FP64 result moves by more than COND_LIMIT under the turn."""
+    from blackhole_b200 import abi
+
+    if moved is None and probe is not None:
+        moved = conditioning(a, probe)
     same = a["what"] == b["what"]
-    out = {"class_agree": float(same.mean()), "against": "the FP64 GPU frame (per ray)"}
+    out = {"class_agree": float(same.mean()), "against": against, "rays": int(len(a)),
+           "class_mismatch": int((~same).sum())}
+    if (~same).any():
+        pairs = {}
+        for wa, wb in zip(a["what"][~same], b["what"][~same]):
+            k = f"{abi.HIT_NAMES[wa]}->{abi.HIT_NAMES[wb]}"
+            pairs[k] = pairs.get(k, 0) + 1
+        out["class_mismatch_pairs"] = pairs
     disc = same & (a["what"] == abi.HIT_DISC) & (a["g"] > 0)
     if disc.any():
         e = np.abs(b["g"][disc] - a["g"][disc]) / a["g"][disc]
-        out["g_rel"] = {"p50": float(np.quantile(e, .5)), "p99": float(np.quantile(e, .99)),
-                        "max": float(e.max()), "frac_le_1e-3": float((e <= 1e-3).mean()), "n": int(disc.sum())}
+        out["g_rel"] = _dist(e, 1e-3)
+        out["g_rel"]["frac_le_1e-3"] = float((e <= 1e-3).mean())
+        if moved is not None:
+            ill = moved[disc] > COND_LIMIT
+            out["g_rel"]["ill_conditioned_rays"] = int(ill.sum())
+            if (~ill).any():
+                out["g_rel"]["max_well_conditioned"] = float(e[~ill].max())
+                out["g_rel"]["n_above_target_well_conditioned"] = int((e[~ill] > 1e-3).sum())
     sky = same & (a["what"] == abi.HIT_SKY)
     if sky.any():
-        d = 2 * np.arcsin(np.clip(np.linalg.norm(b["dir"][sky] - a["dir"][sky], axis=1) / 2, 0, 1))
-        out["dir_rad"] = {"p50": float(np.quantile(d, .5)), "p99": float(np.quantile(d, .99)),
-                          "max": float(d.max()), "frac_le_1e-4": float((d <= 1e-4).mean()), "n": int(sky.sum())}
-        if probe is not None:
-            # kappa: how far the FP64 direction moves when the camera turns by
-            # COND_YAW (a ray that changes class under the turn counts as moved)
-            moved = np.full(int(sky.sum()), np.inf)
-            stay = probe["what"][sky] == abi.HIT_SKY
-            pd = probe["dir"][sky][stay]
-            moved[stay] = 2 * np.arcsin(np.clip(np.linalg.norm(pd - a["dir"][sky][stay], axis=1) / 2, 0, 1))
-            ill = moved > COND_LIMIT
+        d = _angle(b["dir"][sky], a["dir"][sky])
+        out["dir_rad"] = _dist(d, 1e-4)
+        out["dir_rad"]["frac_le_1e-4"] = float((d <= 1e-4).mean())
+        if moved is not None:
+            ill = moved[sky] > COND_LIMIT
             well = d[~ill]
             out["dir_rad"]["conditioning"] = {
-                "probe": "FP64 frame with the camera turned by %.1e rad" % COND_YAW,
+                "probe": "FP64 GPU frame with the camera turned by %.1e rad" % COND_YAW,
                 "ill_conditioned_rays": int(ill.sum()),
-                "their_fp64_move_min": float(moved[ill].min()) if ill.any() else None,
+                "their_fp64_move_min": float(moved[sky][ill].min()) if ill.any() else None,
                 "their_error_max": float(d[ill].max()) if ill.any() else None,
                 "max_well_conditioned": float(well.max()) if well.size else None,
+                "n_above_target_well_conditioned": int((well > 1e-4).sum()),
                 "frac_le_1e-4_well_conditioned": float((well <= 1e-4).mean()) if well.size else None}
     return out
 
 
-def photon_ring_leg(r, torch, flush, barrier, world, rank):
+def rows_of(full, cfg, rows):
+    """The per-sample results of whole rows of a row-major frame."""
+    ss = max(1, cfg.sqrt_spp) ** 2
+    return full.reshape(cfg.height, cfg.width * ss)[np.asarray(rows)].reshape(-1)
+
+
+def checker_pin(r, size):
+    """The GPU frames against the CPU checkers, per ray.  The checkers are
+    test infrastructure used here only to check (nothing measured runs them):
+      - oracle/bh_oracle.c, the FP64 restatement pinned bit for bit to the
+        reference, on every 4th row of the frame under the workload's own
+        settings (uniform sky, r_+(1+1e-6) stop), which the reference lacks;
+      - the reference itself (oracle/_ref) on every 8th row under its own
+        settings (galactic sky, its horizon stop), where it is built.
+    Both precisions of the GPU path are compared; the conditioning probe
+    (FP64 GPU frame, camera turned by COND_YAW) marks ill-conditioned rays."""
+    import copy
+
+    import oracle
+    from blackhole_b200 import abi
+
+    threads = os.cpu_count() or 1
+    out = {}
+
+    def leg(cd, cm, rows, port, checker, settings):
+        t0 = time.perf_counter()
+        chk, _ = port.trace_rows(cd, rows, threads)
+        secs = time.perf_counter() - t0
+        a = rows_of(r.trace_rays(cd), cd, rows)
+        b = rows_of(r.trace_rays(cm), cm, rows)
+        turned = copy.deepcopy(cd)
+        turned.cam.yaw += COND_YAW
+        moved = conditioning(a, rows_of(r.trace_rays(turned), cd, rows))
+        return {"checker": checker, "settings": settings,
+                "sample": f"{len(rows)} rows of the {size}x{size} frame (every {rows[1] - rows[0]}th), "
+                          f"{len(chk)} rays, {threads} threads, {secs:.1f} s",
+                "fp64": compare_rays(chk, a, moved=moved, against=checker),
+                "mixed": compare_rays(chk, b, moved=moved, against=checker),
+                "mixed_vs_fp64_gpu": compare_rays(a, b, moved=moved)}
+
+    cd = frame_config(size, 0, 1, abi.PRECISION_FP64)
+    cm = frame_config(size, 0, 1, abi.PRECISION_MIXED)
+    out["oracle"] = leg(cd, cm, list(range(0, size, 4)), oracle.oracle(),
+                        "the FP64 oracle (oracle/bh_oracle.c)",
+                        "the workload's: uniform sky, horizon stop r_+(1+1e-6)")
+    ref = oracle.reference()
+    if ref is not None:
+        for c in (cd, cm):
+            c.sky_mode = abi.SKY_GALACTIC
+            c.stop_mode = abi.STOP_REFERENCE
+        out["reference"] = leg(cd, cm, list(range(0, size, 8)), ref,
+                               "the reference's own trace()+shade() (oracle/_ref)",
+                               "the reference's: galactic sky, horizon stop r_+ + 1e-4 + 1e-3 (r_+ - r_-)")
+    return out
+
+
+def photon_ring_leg(r, torch, flush, barrier, world, rank, check=True):
     """4096^2 frame of +-8 M centred on the prograde equatorial point of the
     critical curve (a = 0.998, 75 deg): mixed and FP64 device time, the
     per-ray step-count distribution and the mixed-vs-FP64 error."""
@@ -310,6 +408,21 @@ def photon_ring_leg(r, torch, flush, barrier, world, rank):
                          "frac_gt_2000": float((steps > 2000).mean())}
     out["classes"] = {abi.HIT_NAMES[k]: int(v) for k, v in enumerate(np.bincount(a["what"].ravel(), minlength=6))}
     out["accuracy"] = compare_rays(a, b)
+    if rank == 0 and check:
+        # A strip of 16 rows through the frame's centre, which the critical
+        # curve crosses, against the FP64 oracle (the checker, timed apart).
+        import oracle
+
+        rows = list(range(cd.height // 2 - 8, cd.height // 2 + 8))
+        t0 = time.perf_counter()
+        chk, _ = oracle.oracle().trace_rows(cd, rows, os.cpu_count() or 1)
+        secs = time.perf_counter() - t0
+        sa, sb = rows_of(a, cd, rows), rows_of(b, cm, rows)
+        checker = "the FP64 oracle (oracle/bh_oracle.c)"
+        out["accuracy_vs_oracle"] = {
+            "sample": f"rows {rows[0]}..{rows[-1]} ({len(chk)} rays) through the critical curve, {secs:.1f} s",
+            "fp64": compare_rays(chk, sa, against=checker), "mixed": compare_rays(chk, sb, against=checker),
+            "fp64_steps_in_strip": {"mean": float(sa["steps"].mean()), "max": int(sa["steps"].max())}}
     return out
 
 
@@ -515,6 +628,39 @@ def autotune_leg():
                                     "ms": round(st[0].kernel_ms, 3)}}
 
 
+def same_config_leg(r, size, rank, world, steps, warmup, torch, flush, barrier, max_over_ranks):
+    """The same frame on the reference's own sky and horizon stop (the only
+    ones it has; the reference arm times it on them), mixed and FP64: device
+    time and end to end through bh_gpu_render into pinned host memory, so the
+    speed-up over the reference arm can be read like for like."""
+    from blackhole_b200 import abi
+
+    res = {"settings": "galactic-band 250k-star sky (m <= 12) with the Milky Way background, horizon stop "
+                       "r_+ + 1e-4 + 1e-3 (r_+ - r_-): the reference arm's settings"}
+    for name, prec in (("mixed", abi.PRECISION_MIXED), ("fp64", abi.PRECISION_FP64)):
+        cfg = frame_config(size, rank, world, prec)
+        cfg.sky_mode = abi.SKY_GALACTIC
+        cfg.stop_mode = abi.STOP_REFERENCE
+        k = steps if prec == abi.PRECISION_MIXED else max(2, steps // 2)
+        t, _, st, _ = time_device(r, cfg, k, max(1, warmup), torch, flush, barrier)
+        t = max_over_ranks(t)
+        entry = {"value": round(world * cfg.n_rays * k / (t * 1e-3), 1), "unit": "rays/s",
+                 "ms_per_step": round(t / k, 4), "steps_per_ray": round(st.steps / max(1, st.rays), 2)}
+        host = torch.empty((cfg.height, cfg.width, 3), dtype=torch.float64, pin_memory=True).numpy()
+        for _ in range(max(1, warmup)):
+            r.render_into(cfg, host)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            r.render_into(cfg, host)
+        t_e = max_over_ranks(time.perf_counter() - t0)
+        barrier()
+        entry["e2e"] = {"value": round(world * cfg.n_rays * k / t_e, 1), "unit": "rays/s",
+                        "api": "bh_gpu_render (C-ABI) into pinned host memory, wall clock"}
+        res[name] = entry
+    return res
+
+
 def gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -668,6 +814,13 @@ def gpu_arm(args):
         except Exception as e:  # reported, not hidden
             out["display"] = {"error": repr(e)}
 
+    if not args.no_fp64:
+        try:
+            out["same_config_as_reference"] = same_config_leg(r, size, rank, world, args.steps, args.warmup,
+                                                              torch, flush, barrier, max_over_ranks)
+        except Exception as e:  # reported, not hidden
+            out["same_config_as_reference"] = {"error": repr(e)}
+
     # Kernels of ours launched in the timed region per mixed step: the
     # near-critical classification, the binary64 near-critical trace, two
     # binary32 traces (the main grid and the blocks started after the binary64
@@ -697,7 +850,8 @@ def gpu_arm(args):
 
     if not args.no_photon_ring:
         try:
-            out["photon_ring"] = photon_ring_leg(r, torch, flush, barrier, world, rank)
+            out["photon_ring"] = photon_ring_leg(r, torch, flush, barrier, world, rank,
+                                                 check=world == 1 and not args.no_cpu_baseline)
         except Exception as e:  # reported, not hidden
             out["photon_ring"] = {"error": repr(e)}
 
@@ -717,6 +871,10 @@ def gpu_arm(args):
             out["cpu_baseline"] = cpu_baseline(size)
         except Exception as e:
             out["cpu_baseline"] = {"value": None, "error": repr(e)}
+        try:
+            out["accuracy_vs_checkers"] = checker_pin(r, size)
+        except Exception as e:  # reported, not hidden
+            out["accuracy_vs_checkers"] = {"error": repr(e)}
 
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -17,6 +17,11 @@
 // process exits.  All calls share it and it keeps the last call's contents:
 // each call clears the counters that must start at zero, and two calls whose
 // work overlaps on the GPU race on the array, so callers serialise them.
+//
+// The frame constants reach the device as the arguments of a one-block
+// staging kernel, which the launch copies when it is enqueued: no copy reads
+// the host stack after the call returns.  The caller's current device is put
+// back before every return.
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -50,6 +55,43 @@ static_assert(offsetof(bh_trace_record, attempts) == offsetof(HitRecord, attempt
 // device array: its device address comes from cudaGetSymbolAddress, once per
 // device, and only that address is handed to kernels and copies.
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+// The frame constants of a call, the binary64 pass's version of them and the
+// ray count, written with the work-queue counters cleared: one block, its
+// threads copying the two frames a word at a time.
+__global__ void noalloc_stage_kernel(const FrameParams F, const FrameParams G, long long n, QueueState* queue,
+                                     FrameParams* frame, FrameParams* frame_side, long long* ray_end) {
+    static_assert(sizeof(FrameParams) % sizeof(unsigned long long) == 0, "FrameParams is whole words");
+    constexpr int kWords = (int)(sizeof(FrameParams) / sizeof(unsigned long long));
+    const unsigned long long* f = reinterpret_cast<const unsigned long long*>(&F);
+    const unsigned long long* g = reinterpret_cast<const unsigned long long*>(&G);
+    unsigned long long* df = reinterpret_cast<unsigned long long*>(frame);
+    unsigned long long* dg = reinterpret_cast<unsigned long long*>(frame_side);
+    for (int i = threadIdx.x; i < kWords; i += blockDim.x) {
+        df[i] = f[i];
+        dg[i] = g[i];
+    }
+    constexpr int kQueueWords = (int)(sizeof(QueueState) / sizeof(unsigned long long));
+    static_assert(sizeof(QueueState) % sizeof(unsigned long long) == 0, "QueueState is whole words");
+    unsigned long long* dq = reinterpret_cast<unsigned long long*>(queue);
+    for (int i = threadIdx.x; i < kQueueWords; i += blockDim.x) dq[i] = 0ull;
+    if (threadIdx.x == 0) *ray_end = n;
+}
+
+// Puts the calling thread's current device back when the entry point returns.
+struct DeviceRestore {
+    int prev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            cudaGetLastError();
+            prev = -1;
+        }
+    }
+    ~DeviceRestore() {
+        int now = -1;
+        if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+    }
+};
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
@@ -94,6 +136,7 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
         return BH_ERR_NO_DEVICE;
     }
     if (device < 0 || device >= count || device >= kMaxDevices) return BH_ERR_INVALID_ARG;
+    const DeviceRestore restore;
     if (cudaSetDevice(device) != cudaSuccess) return BH_ERR_CUDA;
     unsigned char* base = nullptr;
     if ((rc = scratch_address(device, &base)) != BH_OK) return rc;
@@ -106,12 +149,10 @@ extern "C" int bh_gpu_trace_noalloc(int device, const bh_render_config* cfg, bh_
     long long* ray_end = reinterpret_cast<long long*>(base + kRayEndOff);
     const long long n = F.n_rays;
     // Counters start at zero on every call; the array keeps the last call's.
-    if (cudaMemsetAsync(queue, 0, sizeof(QueueState), s) != cudaSuccess) return BH_ERR_CUDA;
-    if (cudaMemcpyAsync(frame, &F, sizeof F, cudaMemcpyHostToDevice, s) != cudaSuccess) return BH_ERR_CUDA;
     FrameParams* frame_side = reinterpret_cast<FrameParams*>(base + kFrameSideOff);
     const FrameParams G = binary64_treatment(F);
-    if (cudaMemcpyAsync(frame_side, &G, sizeof G, cudaMemcpyHostToDevice, s) != cudaSuccess) return BH_ERR_CUDA;
-    if (cudaMemcpyAsync(ray_end, &n, sizeof n, cudaMemcpyHostToDevice, s) != cudaSuccess) return BH_ERR_CUDA;
+    noalloc_stage_kernel<<<1, 128, 0, s>>>(F, G, n, queue, frame, frame_side, ray_end);
+    if (cudaGetLastError() != cudaSuccess) return BH_ERR_CUDA;
     if (n == 0) return BH_OK;
 
     // The context API's default launch shapes: refill at 32 idle lanes, the

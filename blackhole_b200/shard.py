@@ -7,8 +7,10 @@ into contiguous blocks of nearly equal ray count (the work unit), and
 combines its per-thread stats (render.cpp:481-494): counters summed, drift
 maxima maximised, ``seconds`` the maximum over ranks.  ``reduce_grads`` sums
 the adjoint's loss and four gradients over ranks that each differentiated
-their own frames (the loss of a set of frames is the sum of theirs).  All run
-over any torch.distributed process group (NCCL on GPUs, gloo on CPU).
+their own frames (the loss of a set of frames is the sum of theirs).
+``gather_frames`` brings every rank's frames to one rank, in batch order, as
+the reference's pool joins its rows into one image (render.cpp:474-494).  All
+run over any torch.distributed process group (NCCL on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
@@ -73,4 +75,53 @@ def reduce_grads(grad: dict, group=None, device=None) -> dict:
     out = dict(grad)
     for k, v in zip(keys, t.tolist()):
         out[k] = v if k in GRAD_FIELDS else int(round(v))
+    return out
+
+
+def gather_frames(cfgs: list, mine: list, rank: int, world: int, dst: int = 0, group=None, device=None):
+    """Gather the pixels of a batch sharded by ``frames_for_rank``.
+
+    ``mine`` holds this rank's frames in the order ``frames_for_rank(cfgs,
+    rank, world)`` lists them, each an array of height x width x 3 values
+    (float64 XYZ, or the 8-bit sRGB of a developed frame).  Every rank but
+    ``dst`` sends its frames to ``dst`` as one contiguous buffer (point to
+    point: the frames' sizes differ, and every rank knows them from
+    ``cfgs``).  Returns, on ``dst``, the list of all frames in batch order;
+    None on the other ranks.  ``device``: where the buffers go through the
+    process group (the rank's GPU under NCCL, None for gloo).
+    """
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    if world == 1:
+        return list(mine)
+    parts = [frames_for_rank(cfgs, r, world) for r in range(world)]
+    if len(mine) != len(parts[rank]):
+        raise ValueError(f"rank {rank} holds {len(mine)} frames, frames_for_rank gives it {len(parts[rank])}")
+    dtype = np.asarray(mine[0]).dtype if mine else np.dtype(np.float64)
+    if dtype not in (np.float64, np.uint8):
+        raise ValueError("frames are float64 XYZ or uint8 sRGB")
+    tdt = torch.float64 if dtype == np.float64 else torch.uint8
+    sizes = [cfgs[i].height * cfgs[i].width * 3 for i in range(len(cfgs))]
+    if rank != dst:
+        flat = np.concatenate([np.ascontiguousarray(f, dtype=dtype).reshape(-1) for f in mine]) if mine \
+            else np.zeros(0, dtype=dtype)
+        if flat.size:
+            dist.send(torch.from_numpy(flat).to(device), dst=dst, group=group)
+        return None
+    out = [None] * len(cfgs)
+    for k, i in enumerate(parts[dst]):
+        out[i] = np.ascontiguousarray(mine[k], dtype=dtype).reshape(cfgs[i].height, cfgs[i].width, 3)
+    for r in range(world):
+        if r == dst or not parts[r]:
+            continue
+        n = sum(sizes[i] for i in parts[r])
+        buf = torch.empty(n, dtype=tdt, device=device)
+        dist.recv(buf, src=r, group=group)
+        flat = buf.cpu().numpy()
+        off = 0
+        for i in parts[r]:
+            out[i] = flat[off:off + sizes[i]].reshape(cfgs[i].height, cfgs[i].width, 3)
+            off += sizes[i]
     return out

@@ -375,10 +375,15 @@ typedef struct bh_trace_record {
    statically allocated 6.3 MiB device array of this library, so a call
    takes at most BH_NOALLOC_MAX_RAYS rays and returns BH_ERR_INVALID_ARG
    above that.  Every GPU that loads the library holds the array until exit.
-   The first call on a device looks the array's device address up (do it
-   before any stream capture); every call clears the counters it needs at
-   zero, and all calls share the one array, so calls whose work overlaps on
-   the GPU (other streams, other host threads) race - serialise them.
+   The first call on a device looks the array's device address up, and with
+   CUDA's lazy module loading (the default) it is also the call that loads
+   this library's kernels and places the array on that device, which may
+   allocate and synchronise the device: make that first call once during
+   set-up, outside the real-time path and before any stream capture.  Every
+   call clears the counters it needs at zero, and all calls share the one
+   array, so calls whose work overlaps on the GPU (other streams, other host
+   threads) race - serialise them.  The calling thread's current device is
+   the same on return as on entry.
    A config with a jet returns BH_ERR_UNSUPPORTED (the jet's emission is a
    per-ray sum this entry point has no scratch for).
    Stars, disc temperature and pixels are not computed (no shading): the

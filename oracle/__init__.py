@@ -18,7 +18,10 @@ from blackhole_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "lib", "libbh_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbh_ref.so")
-REF_SRC = "/root/reference/src"
+# The reference's src/ directory: $BH_REFERENCE_SRC, else a checkout named
+# `reference` beside this repository (the same rule as oracle/Makefile).
+REF_SRC = os.environ.get("BH_REFERENCE_SRC") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                             "reference", "src")
 
 _oracle = None
 _ref = None
@@ -73,6 +76,7 @@ def _declare(lib, prefix: str) -> None:
     fn("blackbody_table", None, _PD)
     fn("ray_direction", None, C.POINTER(abi.bh_camera), _D, _D, _D, _PD)
     fn("trace_rays", C.c_int, _CFG, C.c_int, C.c_int, C.c_int, C.c_int, _RR, _ST)
+    fn("trace_rows", C.c_int, _CFG, C.POINTER(C.c_int), C.c_int, C.c_int, _RR, _ST)
     fn("render_window", C.c_int, _CFG, C.c_int, C.c_int, C.c_int, C.c_int,
        C.POINTER(abi.bh_xyz), _ST)
     fn("render", C.c_int, _CFG, C.POINTER(abi.bh_xyz), _ST)
@@ -223,6 +227,23 @@ class Port:
             raise RuntimeError(f"{self.prefix}trace_rays failed: {abi.STATUS_NAMES.get(rc, rc)}")
         arr = np.frombuffer(buf, dtype=abi.ray_result_dtype(), count=n).copy()
         return arr, st
+
+    def trace_rows(self, cfg, rows, threads=0):
+        """Per-sample results of whole rows (in the listed order, each row
+        pixel then sample) on `threads` workers (0: one per host core), plus
+        stats."""
+        c = cfg.to_c() if hasattr(cfg, "to_c") else cfg
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        s = max(1, c.sqrt_spp)
+        n = len(rows) * c.width * s * s
+        buf = (abi.bh_ray_result * max(n, 1))()
+        st = abi.bh_render_stats()
+        threads = threads if threads > 0 else (os.cpu_count() or 1)
+        rc = self._f("trace_rows")(C.byref(c), rows.ctypes.data_as(C.POINTER(C.c_int)), len(rows), threads,
+                                   buf, C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"{self.prefix}trace_rows failed: {abi.STATUS_NAMES.get(rc, rc)}")
+        return np.frombuffer(buf, dtype=abi.ray_result_dtype(), count=n).copy(), st
 
     def render_window(self, cfg, x0=0, y0=0, w=None, h=None):
         c = cfg.to_c() if hasattr(cfg, "to_c") else cfg

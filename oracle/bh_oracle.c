@@ -16,6 +16,7 @@
 #include "bh_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1279,6 +1280,59 @@ static void stats_add(bh_render_stats* s, const bh_render_stats* b) {
     s->max_carter_drift = dmax(s->max_carter_drift, b->max_carter_drift);
 }
 
+/* render.cpp:433-463: the samples of pixel (xx, yy): per-sample results to
+   rays[0 .. S^2) when rays is not NULL, the pixel's average to *pixel when
+   that is not NULL, counters and flux into *local. */
+static void trace_pixel(const scene_t* sc, int xx, int yy, bh_render_stats* local, bh_ray_result* rays,
+                        bh_xyz* pixel) {
+    const bh_render_config* cfg = sc->cfg;
+    const int S = cfg->sqrt_spp > 1 ? cfg->sqrt_spp : 1;
+    const double inv_S = 1.0 / S;
+    rng_t rng = {cfg->seed ^ ((uint64_t)yy << 32) ^ ((uint64_t)xx * 0x9E3779B97F4A7C15ull)};
+    double acc[3] = {0.0, 0.0, 0.0};
+    size_t ridx = 0;
+    for (int sy = 0; sy < S; ++sy) {
+        for (int sx = 0; sx < S; ++sx) {
+            const double jx = (sx + rng_uniform(&rng)) * inv_S;
+            const double jy = (sy + rng_uniform(&rng)) * inv_S;
+            const double u = (2.0 * (xx + jx) / cfg->width - 1.0);
+            const double v = (1.0 - 2.0 * (yy + jy) / cfg->height);
+            double dir[3];
+            ray_direction(&cfg->cam, u, v, sc->aspect, dir);
+            ++local->rays;
+            const hit_t hit = trace(sc, dir, local);
+            double c[3], g, sdir[3];
+            shade_hit(sc, &hit, local, c, &g, sdir);
+            if (hit.jet > 0.0) {   /* render.cpp:384-392 */
+                ++local->jet_rays;
+                c[0] += sc->jet_colour[0] * hit.jet;
+                c[1] += sc->jet_colour[1] * hit.jet;
+                c[2] += sc->jet_colour[2] * hit.jet;
+            }
+            acc[0] += c[0]; acc[1] += c[1]; acc[2] += c[2];
+            if (rays) {
+                bh_ray_result* o = &rays[ridx++];
+                o->what = hit.what;
+                o->steps = hit.steps;
+                memcpy(o->y, hit.y, sizeof hit.y);
+                o->g = g;
+                o->dir[0] = sdir[0]; o->dir[1] = sdir[1]; o->dir[2] = sdir[2];
+                o->xyz.x = c[0]; o->xyz.y = c[1]; o->xyz.z = c[2];
+                o->attempts = hit.attempts;
+                o->reserved = 0;
+                o->max_norm = hit.norm_rel;
+                o->max_q = hit.q_drift;
+                o->jet = hit.jet;
+            }
+        }
+    }
+    const double wgt = 1.0 / (S * S);
+    if (pixel) {
+        pixel->x = acc[0] * wgt; pixel->y = acc[1] * wgt; pixel->z = acc[2] * wgt;
+    }
+    local->total_flux += acc[1] * wgt;
+}
+
 /* render.cpp:428-463: the pixel loop over a window, one result per sample. */
 static int run_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                       bh_ray_result* rays, bh_xyz* pixels, bh_render_stats* stats) {
@@ -1292,56 +1346,82 @@ static int run_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
     bh_render_stats local;
     memset(&local, 0, sizeof local);
     const int S = cfg->sqrt_spp > 1 ? cfg->sqrt_spp : 1;
-    const double inv_S = 1.0 / S;
     size_t ridx = 0;
     for (int yy = y0; yy < y0 + h; ++yy) {
         for (int xx = x0; xx < x0 + w; ++xx) {
-            rng_t rng = {cfg->seed ^ ((uint64_t)yy << 32) ^ ((uint64_t)xx * 0x9E3779B97F4A7C15ull)};
-            double acc[3] = {0.0, 0.0, 0.0};
-            for (int sy = 0; sy < S; ++sy) {
-                for (int sx = 0; sx < S; ++sx) {
-                    const double jx = (sx + rng_uniform(&rng)) * inv_S;
-                    const double jy = (sy + rng_uniform(&rng)) * inv_S;
-                    const double u = (2.0 * (xx + jx) / cfg->width - 1.0);
-                    const double v = (1.0 - 2.0 * (yy + jy) / cfg->height);
-                    double dir[3];
-                    ray_direction(&cfg->cam, u, v, sc.aspect, dir);
-                    ++local.rays;
-                    const hit_t hit = trace(&sc, dir, &local);
-                    double c[3], g, sdir[3];
-                    shade_hit(&sc, &hit, &local, c, &g, sdir);
-                    if (hit.jet > 0.0) {   /* render.cpp:384-392 */
-                        ++local.jet_rays;
-                        c[0] += sc.jet_colour[0] * hit.jet;
-                        c[1] += sc.jet_colour[1] * hit.jet;
-                        c[2] += sc.jet_colour[2] * hit.jet;
-                    }
-                    acc[0] += c[0]; acc[1] += c[1]; acc[2] += c[2];
-                    if (rays) {
-                        bh_ray_result* o = &rays[ridx++];
-                        o->what = hit.what;
-                        o->steps = hit.steps;
-                        memcpy(o->y, hit.y, sizeof hit.y);
-                        o->g = g;
-                        o->dir[0] = sdir[0]; o->dir[1] = sdir[1]; o->dir[2] = sdir[2];
-                        o->xyz.x = c[0]; o->xyz.y = c[1]; o->xyz.z = c[2];
-                        o->attempts = hit.attempts;
-                        o->reserved = 0;
-                        o->max_norm = hit.norm_rel;
-                        o->max_q = hit.q_drift;
-                        o->jet = hit.jet;
-                    }
-                }
-            }
-            const double wgt = 1.0 / (S * S);
-            if (pixels) {
-                bh_xyz* p = &pixels[(size_t)(yy - y0) * w + (xx - x0)];
-                p->x = acc[0] * wgt; p->y = acc[1] * wgt; p->z = acc[2] * wgt;
-            }
-            local.total_flux += acc[1] * wgt;
+            trace_pixel(&sc, xx, yy, &local, rays ? &rays[ridx] : NULL,
+                        pixels ? &pixels[(size_t)(yy - y0) * w + (xx - x0)] : NULL);
+            ridx += (size_t)S * S;
         }
     }
     if (stats) stats_add(stats, &local);
+    scene_free(&sc);
+    return BH_OK;
+}
+
+/* The pixel loop over a list of whole rows on `threads` workers, each taking
+   the next row from a shared counter (render.cpp:420-477's pool, for
+   per-sample results of large parts of a frame).  Samples of the k-th listed
+   row go to out[(k * width + x) * S^2 + s]. */
+typedef struct {
+    const scene_t* sc;
+    const int* rows;
+    int nrows;
+    int next;
+    pthread_mutex_t lock;
+    bh_ray_result* out;
+    bh_render_stats stats;
+} rows_job_t;
+
+static void* rows_worker(void* arg) {
+    rows_job_t* job = (rows_job_t*)arg;
+    const bh_render_config* cfg = job->sc->cfg;
+    const int S = cfg->sqrt_spp > 1 ? cfg->sqrt_spp : 1;
+    bh_render_stats local;
+    memset(&local, 0, sizeof local);
+    for (;;) {
+        pthread_mutex_lock(&job->lock);
+        const int k = job->next++;
+        pthread_mutex_unlock(&job->lock);
+        if (k >= job->nrows) break;
+        for (int xx = 0; xx < cfg->width; ++xx)
+            trace_pixel(job->sc, xx, job->rows[k], &local,
+                        &job->out[((size_t)k * cfg->width + xx) * S * S], NULL);
+    }
+    pthread_mutex_lock(&job->lock);
+    stats_add(&job->stats, &local);
+    pthread_mutex_unlock(&job->lock);
+    return NULL;
+}
+
+int orc_trace_rows(const bh_render_config* cfg, const int* rows, int nrows, int threads, bh_ray_result* out,
+                   bh_render_stats* stats) {
+    if (!cfg || nrows < 0 || (nrows > 0 && (!rows || !out))) return BH_ERR_INVALID_ARG;
+    for (int k = 0; k < nrows; ++k)
+        if (rows[k] < 0 || rows[k] >= cfg->height) return BH_ERR_INVALID_ARG;
+    scene_t sc;
+    int rc = scene_init(&sc, cfg);
+    if (rc != BH_OK) return rc;
+    table_build();   /* the lazily built blackbody table, before any worker reads it */
+    rows_job_t job;
+    memset(&job, 0, sizeof job);
+    job.sc = &sc;
+    job.rows = rows;
+    job.nrows = nrows;
+    job.out = out;
+    pthread_mutex_init(&job.lock, NULL);
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    pthread_t tid[256];
+    int started = 0;
+    for (int t = 0; t < threads; ++t) {
+        if (pthread_create(&tid[t], NULL, rows_worker, &job) != 0) break;
+        ++started;
+    }
+    if (started == 0) rows_worker(&job);
+    for (int t = 0; t < started; ++t) pthread_join(tid[t], NULL);
+    pthread_mutex_destroy(&job.lock);
+    if (stats) stats_add(stats, &job.stats);
     scene_free(&sc);
     return BH_OK;
 }

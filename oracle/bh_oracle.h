@@ -74,6 +74,10 @@ void   orc_ray_direction(const bh_camera* cam, double sx, double sy, double aspe
    [x0, x0+w) x [y0, y0+h), ordered by pixel then sample, as bh_gpu_trace_rays. */
 int    orc_trace_rays(const bh_render_config* cfg, int x0, int y0, int w, int h,
                       bh_ray_result* out, bh_render_stats* stats);
+/* Per-sample results of whole rows (rows[0..nrows)) on `threads` workers:
+   sample s of pixel x of the k-th listed row at out[(k * width + x) * S^2 + s]. */
+int    orc_trace_rows(const bh_render_config* cfg, const int* rows, int nrows, int threads,
+                      bh_ray_result* out, bh_render_stats* stats);
 /* Pixels of the same window (w*h, row-major).  stats are added into. */
 int    orc_render_window(const bh_render_config* cfg, int x0, int y0, int w, int h,
                          bh_xyz* out, bh_render_stats* stats);

@@ -251,6 +251,91 @@ int ref_render_rows(const bh_render_config* c, const int* rows, int nrows, int t
     return BH_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The samples of pixel (x, y) through the reference's trace() and shade():
+// per-sample results into out[0 .. S^2), counters and flux into `local`.
+void trace_pixel(const Scene& sc, int x, int y, bh::RenderStats& local, bh_ray_result* out) {
+    const bh::RenderConfig& cfg = sc.cfg;
+    const int S = std::max(1, cfg.sqrt_spp);
+    const double inv_S = 1.0 / S;
+    size_t idx = 0;
+    bh::Rng rng(cfg.seed ^ (static_cast<uint64_t>(y) << 32) ^
+                (static_cast<uint64_t>(x) * 0x9E3779B97F4A7C15ull));
+    spec::XYZ acc{};
+    for (int sy = 0; sy < S; ++sy)
+        for (int sx = 0; sx < S; ++sx) {
+            const double jx = (sx + rng.uniform()) * inv_S;
+            const double jy = (sy + rng.uniform()) * inv_S;
+            const double u = (2.0 * (x + jx) / cfg.width - 1.0);
+            const double v = (1.0 - 2.0 * (y + jy) / cfg.height);
+            double dir[3];
+            cfg.cam.ray_direction(u, v, sc.aspect, dir);
+            ++local.rays;
+            bh::RenderStats rs;   // this ray's own counters and drift maxima
+            const bh::Hit hit = bh::trace(cfg, sc.disc.get(), dir, sc.tet, rs);
+            local.steps += rs.steps;
+            local.max_norm_error = std::max(local.max_norm_error, rs.max_norm_error);
+            local.max_carter_drift = std::max(local.max_carter_drift, rs.max_carter_drift);
+            const spec::XYZ col = bh::shade(cfg, sc.disc.get(), sc.stars.get(), hit,
+                                            sc.psf_sigma, sc.jet_colour, local);
+            acc.x += col.x; acc.y += col.y; acc.z += col.z;
+            bh_ray_result& o = out[idx++];
+            std::memset(&o, 0, sizeof o);
+            o.what = static_cast<int32_t>(hit.what);
+            o.steps = static_cast<int32_t>(rs.steps);
+            o.max_norm = rs.max_norm_error;
+            o.max_q = rs.max_carter_drift;
+            o.jet = hit.jet;
+            for (int i = 0; i < 8; ++i) o.y[i] = hit.y[i];
+            o.xyz.x = col.x; o.xyz.y = col.y; o.xyz.z = col.z;
+            // The fields shade_hit computes on the way (render.cpp:275-325).
+            if (hit.what == bh::Hit::What::Disc && sc.disc) {
+                const double r = hit.y[bh::Y_R];
+                if (sc.disc->temperature(r) > 0.0) {
+                    const double g = bh::redshift_factor(hit.y, sc.disc->four_velocity(r));
+                    o.g = (g > 0.0) ? g : 0.0;
+                }
+            } else if (hit.what == bh::Hit::What::Sky) {
+                const bh::State d = bh::geodesic_rhs(cfg.spin, hit.y);
+                double v3[3];
+                bh::cartesian_velocity(cfg.spin, hit.y, d, v3);
+                const double vn = std::sqrt(v3[0] * v3[0] + v3[1] * v3[1] + v3[2] * v3[2]);
+                if (vn > 0.0)
+                    for (int i = 0; i < 3; ++i) o.dir[i] = v3[i] / vn;
+            } else if (hit.what == bh::Hit::What::Sun) {
+                const bh::Geom gm = bh::geom_at(cfg.spin, hit.y[bh::Y_R], hit.y[bh::Y_TH]);
+                const bh::MetricLower ml = bh::metric_lower(gm);
+                if (ml.tt < 0.0) {
+                    const std::array<double, 4> u = {1.0 / std::sqrt(-ml.tt), 0.0, 0.0, 0.0};
+                    const double g = bh::redshift_factor(hit.y, u);
+                    o.g = (g > 0.0) ? g : 0.0;
+                }
+            } else if (hit.what == bh::Hit::What::Star) {
+                const auto u = cfg.star.surface_four_velocity(hit.y[bh::Y_TH]);
+                const double ku = hit.y[bh::Y_PT] * u[0] + hit.y[bh::Y_PPH] * u[3];
+                if (ku > 1e-12) o.g = 1.0 / ku;
+            }
+        }
+    const double w = 1.0 / (S * S);
+    local.total_flux += acc.y * w;
+}
+
+void add_stats(bh::RenderStats& total, const bh::RenderStats& s) {
+    total.rays += s.rays; total.steps += s.steps; total.captured += s.captured;
+    total.disc_hits += s.disc_hits; total.sun_hits += s.sun_hits; total.star_hits += s.star_hits;
+    total.jet_rays += s.jet_rays; total.escaped += s.escaped; total.exhausted += s.exhausted;
+    total.total_flux += s.total_flux;
+    total.max_norm_error = std::max(total.max_norm_error, s.max_norm_error);
+    total.max_carter_drift = std::max(total.max_carter_drift, s.max_carter_drift);
+}
+
+}  // namespace
+
+extern "C" {
+
 // Per-sample trace()/shade() results of a pixel window, single-threaded.
 int ref_trace_rays(const bh_render_config* c, int x0, int y0, int w, int h, bh_ray_result* out,
                    bh_render_stats* st) {
@@ -259,74 +344,50 @@ int ref_trace_rays(const bh_render_config* c, int x0, int y0, int w, int h, bh_r
     if (x0 < 0 || y0 < 0 || w < 0 || h < 0 || x0 + w > c->width || y0 + h > c->height)
         return BH_ERR_INVALID_ARG;
     Scene sc(*c, c->milky_way != 0);
-    const bh::RenderConfig& cfg = sc.cfg;
     bh::RenderStats local;
-    const int S = std::max(1, cfg.sqrt_spp);
-    const double inv_S = 1.0 / S;
+    const int S = std::max(1, sc.cfg.sqrt_spp);
     size_t idx = 0;
     for (int y = y0; y < y0 + h; ++y)
         for (int x = x0; x < x0 + w; ++x) {
-            bh::Rng rng(cfg.seed ^ (static_cast<uint64_t>(y) << 32) ^
-                        (static_cast<uint64_t>(x) * 0x9E3779B97F4A7C15ull));
-            spec::XYZ acc{};
-            for (int sy = 0; sy < S; ++sy)
-                for (int sx = 0; sx < S; ++sx) {
-                    const double jx = (sx + rng.uniform()) * inv_S;
-                    const double jy = (sy + rng.uniform()) * inv_S;
-                    const double u = (2.0 * (x + jx) / cfg.width - 1.0);
-                    const double v = (1.0 - 2.0 * (y + jy) / cfg.height);
-                    double dir[3];
-                    cfg.cam.ray_direction(u, v, sc.aspect, dir);
-                    ++local.rays;
-                    bh::RenderStats rs;   // this ray's own counters and drift maxima
-                    const bh::Hit hit = bh::trace(cfg, sc.disc.get(), dir, sc.tet, rs);
-                    local.steps += rs.steps;
-                    local.max_norm_error = std::max(local.max_norm_error, rs.max_norm_error);
-                    local.max_carter_drift = std::max(local.max_carter_drift, rs.max_carter_drift);
-                    const spec::XYZ col = bh::shade(cfg, sc.disc.get(), sc.stars.get(), hit,
-                                                    sc.psf_sigma, sc.jet_colour, local);
-                    acc.x += col.x; acc.y += col.y; acc.z += col.z;
-                    bh_ray_result& o = out[idx++];
-                    std::memset(&o, 0, sizeof o);
-                    o.what = static_cast<int32_t>(hit.what);
-                    o.steps = static_cast<int32_t>(rs.steps);
-                    o.max_norm = rs.max_norm_error;
-                    o.max_q = rs.max_carter_drift;
-                    o.jet = hit.jet;
-                    for (int i = 0; i < 8; ++i) o.y[i] = hit.y[i];
-                    o.xyz.x = col.x; o.xyz.y = col.y; o.xyz.z = col.z;
-                    // The fields shade_hit computes on the way (render.cpp:275-325).
-                    if (hit.what == bh::Hit::What::Disc && sc.disc) {
-                        const double r = hit.y[bh::Y_R];
-                        if (sc.disc->temperature(r) > 0.0) {
-                            const double g = bh::redshift_factor(hit.y, sc.disc->four_velocity(r));
-                            o.g = (g > 0.0) ? g : 0.0;
-                        }
-                    } else if (hit.what == bh::Hit::What::Sky) {
-                        const bh::State d = bh::geodesic_rhs(cfg.spin, hit.y);
-                        double v3[3];
-                        bh::cartesian_velocity(cfg.spin, hit.y, d, v3);
-                        const double vn = std::sqrt(v3[0] * v3[0] + v3[1] * v3[1] + v3[2] * v3[2]);
-                        if (vn > 0.0)
-                            for (int i = 0; i < 3; ++i) o.dir[i] = v3[i] / vn;
-                    } else if (hit.what == bh::Hit::What::Sun) {
-                        const bh::Geom gm = bh::geom_at(cfg.spin, hit.y[bh::Y_R], hit.y[bh::Y_TH]);
-                        const bh::MetricLower ml = bh::metric_lower(gm);
-                        if (ml.tt < 0.0) {
-                            const std::array<double, 4> u = {1.0 / std::sqrt(-ml.tt), 0.0, 0.0, 0.0};
-                            const double g = bh::redshift_factor(hit.y, u);
-                            o.g = (g > 0.0) ? g : 0.0;
-                        }
-                    } else if (hit.what == bh::Hit::What::Star) {
-                        const auto u = cfg.star.surface_four_velocity(hit.y[bh::Y_TH]);
-                        const double ku = hit.y[bh::Y_PT] * u[0] + hit.y[bh::Y_PPH] * u[3];
-                        if (ku > 1e-12) o.g = 1.0 / ku;
-                    }
-                }
-            const double w = 1.0 / (S * S);
-            local.total_flux += acc.y * w;
+            trace_pixel(sc, x, y, local, out + idx);
+            idx += static_cast<size_t>(S) * S;
         }
     stats_out(local, st);
+    return BH_OK;
+}
+
+// Per-sample results of whole rows on `threads` workers pulling rows from an
+// atomic counter, as render() shares rows out (render.cpp:420-477): sample s
+// of pixel x of the k-th listed row at out[(k * width + x) * S^2 + s].
+int ref_trace_rows(const bh_render_config* c, const int* rows, int nrows, int threads, bh_ray_result* out,
+                   bh_render_stats* st) {
+    const int rc = check_cfg(c);
+    if (rc != BH_OK) return rc;
+    if (nrows < 0 || (nrows > 0 && (!rows || !out))) return BH_ERR_INVALID_ARG;
+    for (int k = 0; k < nrows; ++k)
+        if (rows[k] < 0 || rows[k] >= c->height) return BH_ERR_INVALID_ARG;
+    Scene sc(*c, c->milky_way != 0);
+    (void)spec::blackbody_xyz(5000.0);  // the magic-static table, before the workers
+    int nthreads = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
+    if (nthreads <= 0) nthreads = 1;
+    const int S = std::max(1, sc.cfg.sqrt_spp);
+    std::atomic<int> next{0};
+    std::vector<bh::RenderStats> per_thread(nthreads);
+    auto worker = [&](int tid) {
+        for (;;) {
+            const int k = next.fetch_add(1);
+            if (k >= nrows) break;
+            for (int x = 0; x < sc.cfg.width; ++x)
+                trace_pixel(sc, x, rows[k], per_thread[tid],
+                            out + (static_cast<size_t>(k) * sc.cfg.width + x) * S * S);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t) pool.emplace_back(worker, t);
+    for (auto& th : pool) th.join();
+    bh::RenderStats total;
+    for (const auto& s : per_thread) add_stats(total, s);
+    stats_out(total, st);
     return BH_OK;
 }
 

@@ -1,8 +1,9 @@
 """Multi-rank frame sharding and stats reduction, on CPU with gloo.
 
-The render path shards by frame with no data-path collective; the only
-cross-rank step is the stats reduction (sums and maxima) and the timing max.
-Two gloo ranks on 127.0.0.1 run the same code bench.py runs over NCCL.
+The render path shards by frame with no data-path collective; the cross-rank
+steps are the stats reduction (sums and maxima), the timing max and the final
+gather of every rank's frames to one rank.  Two gloo ranks on 127.0.0.1 run
+the same code bench.py runs over NCCL.
 """
 import os
 import socket
@@ -10,8 +11,10 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
+import numpy as np
+
 from blackhole_b200 import shard, workloads
-from blackhole_b200.config import RenderStats
+from blackhole_b200.config import RenderConfig, RenderStats
 
 
 def test_partition_covers_every_frame_once_and_balances_rays():
@@ -81,3 +84,59 @@ def test_two_gloo_ranks_reduce_stats_and_split_frames():
         assert tot["seconds"] == pytest.approx(1.5) and tot["total_flux"] == pytest.approx(4.5)
     a, b = res[0][2], res[1][2]
     assert sorted(a + b) == list(range(64)) and not set(a) & set(b)
+
+
+def _small_batch():
+    """Seven frames of uneven size (the batch's shape, CPU-sized)."""
+    dims = [(24, 16), (8, 8), (40, 30), (16, 9), (32, 32), (12, 20), (48, 27)]
+    return [RenderConfig(width=w, height=h) for w, h in dims]
+
+
+def _fake_frame(cfg, i, kind):
+    """A frame's pixels as a deterministic function of frame and pixel: the
+    stand-in for a render, so the test checks the gather's bookkeeping."""
+    n = cfg.height * cfg.width * 3
+    v = (np.arange(n, dtype=np.float64) * 1.25 + 1000.0 * i).reshape(cfg.height, cfg.width, 3)
+    return v if kind == "xyz" else (v.astype(np.int64) % 251).astype(np.uint8)
+
+
+def _gather_worker(rank, world, port, q, kind):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    cfgs = _small_batch()
+    mine = [_fake_frame(cfgs[i], i, kind) for i in shard.frames_for_rank(cfgs, rank, world)]
+    got = shard.gather_frames(cfgs, mine, rank, world)
+    q.put((rank, got))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind", ["xyz", "srgb8"])
+def test_two_gloo_ranks_gather_frames_equal_one_rank_batch(kind):
+    cfgs = _small_batch()
+    single = shard.gather_frames(cfgs, [_fake_frame(c, i, kind) for i, c in enumerate(cfgs)], 0, 1)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, q, kind)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[1] is None
+    assert len(res[0]) == len(cfgs)
+    for a, b, c in zip(res[0], single, cfgs):
+        assert a.shape == (c.height, c.width, 3) and a.dtype == b.dtype
+        assert np.array_equal(a, b)
+
+
+def test_gather_rejects_a_wrong_frame_count():
+    cfgs = _small_batch()
+    with pytest.raises(ValueError):
+        shard.gather_frames(cfgs, [], 0, 2)
