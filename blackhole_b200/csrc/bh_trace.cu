@@ -155,11 +155,15 @@ struct Aux {
 constexpr double kMaxShift = 0.25;
 
 __device__ __forceinline__ void shift_sincos(float s0, float c0, float d, float* s, float* c) {
+    // sin d = d + d^3 (-1/6 + d^2 (1/120 - d^2 / 5040)),
+    // cos d = 1 + d^2 (-1/2 + d^2 (1/24 - d^2 / 720)), in Horner form
     const float d2 = d * d;
-    const float sd = d * (1.f - d2 * (1.f / 6.f) * (1.f - d2 * (1.f / 20.f) * (1.f - d2 * (1.f / 42.f))));
-    const float cd = 1.f - d2 * 0.5f * (1.f - d2 * (1.f / 12.f) * (1.f - d2 * (1.f / 30.f)));
-    *s = s0 * cd + c0 * sd;
-    *c = c0 * cd - s0 * sd;
+    const float ps = fmaf(d2, fmaf(d2, -1.f / 5040.f, 1.f / 120.f), -1.f / 6.f);
+    const float pc = fmaf(d2, fmaf(d2, -1.f / 720.f, 1.f / 24.f), -0.5f);
+    const float sd = fmaf(d * d2, ps, d);
+    const float cd = fmaf(d2, pc, 1.f);
+    *s = fmaf(s0, cd, c0 * sd);
+    *c = fmaf(c0, cd, -(s0 * sd));
 }
 __device__ __forceinline__ void shift_sincos(double s0, double c0, double d, double* s, double* c) {
     // reciprocals as constants: a division by 6.0 is a real division
@@ -176,6 +180,38 @@ __device__ __forceinline__ void shift_sincos(double s0, double c0, double d, dou
     *c = c0 * cd - s0 * sd;
 }
 
+// ---- packed binary32 pairs ----------------------------------------------------
+// sm_100's f32x2 arithmetic: one instruction does the same binary32 operation,
+// rounded to nearest, on the two halves of a 64-bit register pair.  The mixed
+// kernel pairs independent operations of one ray: in the right-hand side,
+// and in the stage sums, which run on the six components as three pairs in
+// the order and with the roundings of the scalar form (product, then fused
+// multiply-adds, then the fused y + h * sum).
+using u64 = unsigned long long;
+__device__ __forceinline__ u64 pk2(float lo, float hi) {
+    u64 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void up2(u64 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+    u64 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ u64 mul2(u64 a, u64 b) {
+    u64 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 sub2(u64 a, u64 b) {
+    u64 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
 // Hamilton's equations for H = 1/2 g^{mu nu} p_mu p_nu (geodesic.h:50-71),
 // with the Kerr inverse metric in Carter's separated form
 //   2 Sigma H = Delta p_r^2 + p_th^2 + (L_z - a E sin^2)^2 / sin^2
@@ -186,11 +222,72 @@ __device__ __forceinline__ void shift_sincos(double s0, double c0, double d, dou
 // not imposed (B is the full bracket).  Delta = (r - r_+)(r - r_-) with each
 // factor formed against a two-term r_+-, so the factor that vanishes at the
 // horizon is exact.  sn, cs: sin and cos of th.
+//
+// The binary32 form pairs the independent products and sums in f32x2
+// instructions (the same operations, grouped two by two; d4 and d5 with their
+// terms gathered as -iS/2 (Dr (p_r^2 + KiD^2) - 2 r (2 E KiD + B iS)) and
+// -sin cos iS (a^2 E^2 - L_z^2 isn2^2 + a^2 B iS)).
+__device__ __forceinline__ void rhs_sc_x2(const Lane<Mixed>& L, float r, float sn, float cs, float pr, float pth,
+                                          float* d, Aux<Mixed>* aux) {
+    if (fabsf(sn) < 1e-9f) sn = (sn < 0.f) ? -1e-9f : 1e-9f;        // kerr.h:51
+    float sn2, cs2;
+    up2(mul2(pk2(sn, cs), pk2(sn, cs)), sn2, cs2);
+    const float r2 = r * r;
+    const float S = fmaf(L.a2R, cs2, r2);
+    float D;
+    if (L.factored) {
+        float f1, f2;
+        up2(sub2(sub2(pk2(r, r), pk2(L.rp_hi, L.rm_hi)), pk2(L.rp_lo, L.rm_lo)), f1, f2);
+        D = f1 * f2;
+    } else {
+        D = r2 - 2.f * r + L.a2R;
+    }
+    const float SD = S * D;
+    const float inv = Mixed::rcp(SD * sn2);
+    float iS, iD;
+    up2(mul2(mul2(pk2(D, S), pk2(sn2, sn2)), pk2(inv, inv)), iS, iD);
+    const float isn2 = inv * SD;
+    const float r2a2 = r2 + L.a2R;
+    float K, Lp;                                       // (r^2+a^2) E - a L_z, L_z - a E sin^2
+    up2(fma2(pk2(r2a2, -L.aE), pk2(L.E, sn2), pk2(-L.aLz, L.Lz)), K, Lp);
+    const float KiD = K * iD;
+    float Dpr, Lpi;                                    // Delta p_r, Lp isn2
+    up2(mul2(pk2(D, Lp), pk2(pr, isn2)), Dpr, Lpi);
+    float m1, m2;                                      // p_th^2, -K KiD
+    up2(mul2(pk2(pth, -K), pk2(pth, KiD)), m1, m2);
+    float b1, b2;
+    up2(fma2(pk2(Dpr, Lpi), pk2(pr, Lp), pk2(m1, m2)), b1, b2);
+    const float B = b1 + b2;
+    float u0, u3;
+    up2(fma2(pk2(r2a2, L.aR), pk2(KiD, KiD), pk2(L.aR * Lp, Lpi)), u0, u3);
+    up2(mul2(pk2(u0, u3), pk2(iS, iS)), d[0], d[3]);
+    up2(mul2(pk2(Dpr, pth), pk2(iS, iS)), d[1], d[2]);
+    const float BiS = B * iS;
+    float p2, k2;
+    up2(mul2(pk2(pr, KiD), pk2(pr, KiD)), p2, k2);
+    const float Dr = fmaf(2.f, r, -2.f);
+    const float Q = fmaf(2.f * L.E, KiD, BiS);
+    const float in4 = fmaf(Dr, p2 + k2, -2.f * r * Q);
+    const float in5 = fmaf(L.a2R, BiS, fmaf(-L.Lz2, isn2 * isn2, L.a2E2));
+    up2(mul2(pk2(-0.5f * iS, -(sn * cs) * iS), pk2(in4, in5)), d[4], d[5]);
+    if (aux) {
+        aux->sn = sn;
+        aux->cs = cs;
+        aux->sn2 = sn2;
+        aux->cs2 = cs2;
+        aux->D = D;
+    }
+}
+
 template <class P>
 __device__ __forceinline__ void rhs_sc(const Lane<P>& L, typename P::R r, typename P::R sn,
                                        typename P::R cs, typename P::R pr, typename P::R pth,
                                        typename P::R* d, Aux<P>* aux) {
     using R = typename P::R;
+    if constexpr (P::kMixed) {
+        rhs_sc_x2(L, r, sn, cs, pr, pth, d, aux);
+        return;
+    }
     if (fabs(sn) < R(1e-9)) sn = (sn < R(0)) ? R(-1e-9) : R(1e-9);   // kerr.h:51
     const R sn2 = sn * sn, cs2 = cs * cs;
     const R r2 = r * r;
@@ -246,31 +343,6 @@ __device__ __forceinline__ void rhs_stage(const Lane<P>& L, typename P::R r, typ
 }
 
 
-// ---- packed binary32 pairs ----------------------------------------------------
-// sm_100's f32x2 arithmetic: one instruction does the same binary32 operation,
-// rounded to nearest, on the two halves of a 64-bit register pair.  The stage
-// sums of the mixed kernel run on the six components as three pairs, in the
-// order and with the roundings of the scalar form (product, then fused
-// multiply-adds, then the fused y + h * sum).
-using u64 = unsigned long long;
-__device__ __forceinline__ u64 pk2(float lo, float hi) {
-    u64 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ void up2(u64 v, float& lo, float& hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
-    u64 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ u64 mul2(u64 a, u64 b) {
-    u64 d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
 // sum_s c[s] k_s[i] for the component pair (2j, 2j+1).
 template <int N>
 __device__ __forceinline__ u64 stage_sum_f2(int j, const float (&c)[N], const float* const (&k)[N]) {
@@ -647,10 +719,15 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
                               : h * (R(E1) * L.k1[i] + R(E3) * k3[i] + R(E4) * k4[i] + R(E5) * k5[i] +
                                      R(E6) * k6[i] + R(E7) * k7[i]);
         if (P::kMixed) {
-            // the scale of the true angle where the lane holds its mirror
+            // the scale of the true angle where the lane holds its mirror;
+            // the azimuth's scale is atol + rtol, whatever its value: an
+            // angle's error does not grow with the distance from phi = 0
+            // (under the reference's |phi| scale a camera at phi = 0 takes
+            // more steps than the same scene turned about the axis)
             const float y0 = (i == 2 && L.mirror) ? kPiHi - (float)L.y[i] : (float)L.y[i];
             const float y1 = (i == 2 && L.mirror) ? kPiHi - (float)yn[i] : (float)yn[i];
-            const float sc = (float)F.atol + (float)F.rtol * fmaxf(fabsf(y0), fabsf(y1));
+            const float sc = (i == 3) ? (float)F.atol + (float)F.rtol
+                                      : (float)F.atol + (float)F.rtol * fmaxf(fabsf(y0), fabsf(y1));
             const float q = (float)e * Mixed::rcp(sc);
             err2f += q * q;
         } else {
