@@ -48,9 +48,11 @@ def test_adapter_renders_the_reference_frame():
     assert abs(st.steps - rs.steps) / rs.steps < 0.01
 
 
-def test_adapter_mixed_precision_meets_the_target_on_the_frame():
+def test_adapter_mixed_precision_is_the_libraries_mixed_frame():
     lib = adapter()
     cfg = workloads.kerr_fp64_256()
+    cfg.sky_mode = abi.SKY_GALACTIC      # bh::RenderConfig has the reference's sky and stop only
+    cfg.stop_mode = abi.STOP_REFERENCE
     c = cfg.to_c()
     via = np.zeros((cfg.height, cfg.width, 3))
     st = abi.bh_render_stats()
