@@ -25,6 +25,8 @@ struct FrameParams {
     double hmax_a, hmax_b;           // step cap hmax_a max(1, r - r_h) + hmax_b (render.cpp:130-131)
     double rtol_ref, atol_ref;       // the binary64 path's tolerances (the config's rtol, atol)
     double r_promote;                // innermost photon orbit: an ingoing ray below it is falling in
+    double land_limit, land_target;  // mixed: a step from inside r_escape that would end beyond land_limit
+                                     // is shortened to end near land_target (see land_escape)
     int32_t early_capture;           // mixed: end such a ray as captured there
     int32_t mirror_ok;               // mixed: integrate th > pi/2 as its mirror pi - th
     int32_t fp64_near_critical;      // mixed: near-critical rays traced in binary64
@@ -84,7 +86,7 @@ struct FrameParams {
     double hs_r, hs_phi0, hs_sigma, hs_contrast, hs_omega;
     double observer_time;
     int32_t precision_tag;           // BH_PRECISION_* of the launch
-    int32_t pad3;
+    int32_t land_escape;             // mixed: land the escaping step within the reference's cap of r_escape
 
     // ---- jet (jet.h:96-315; sampled per step, render.cpp:107-122) ------------
     int32_t jet_enabled;

@@ -30,6 +30,8 @@ constexpr double kMixedAtolFloor = 1e-8;
 // The reference's step cap hmax = kHmaxA max(1, r - r_h) + kHmaxB (render.cpp:130-131).
 constexpr double kHmaxA = 0.05;
 constexpr double kHmaxB = 0.01;
+// The mixed path's own step cap, kHmaxLoose max(1, r - r_h), where it drops the reference's.
+constexpr double kHmaxLoose = 0.3;
 
 double clampd(double v, double lo, double hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
 double maxd(double a, double b) { return (a < b) ? b : a; }
@@ -348,8 +350,28 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     const bool needs_cap = c.sun_enabled || c.star.enabled || c.jet_enabled;
     const bool capped = c.precision != BH_PRECISION_MIXED || c.mixed_step_limit == BH_STEP_LIMIT_REFERENCE ||
                         (c.mixed_step_limit == BH_STEP_LIMIT_AUTO && needs_cap);
-    F.hmax_a = capped ? kHmaxA : 1e30;
-    F.hmax_b = capped ? kHmaxB : 1e30;
+    // Without the reference's cap the mixed path keeps a looser one,
+    // h <= 0.3 max(1, r - r_h): far out the error control alone lets the
+    // step grow past the scale on which the strong field sets in, and the
+    // attempts that overshoot are rejected.  Measured on the CPU
+    // restatement at rtol 1e-6 (edge-on frame, every 32nd row): 58.4 attempts
+    // per ray instead of 64.9 (with 50.9 accepted steps instead of 51.3),
+    // the direction error unchanged (p99 2.6e-6 rad); over 120 random scenes
+    // 8% fewer attempts and fewer rays beyond 1e-4 rad.  BH_STEP_LIMIT_NONE
+    // leaves the error control alone.
+    const bool none = c.precision == BH_PRECISION_MIXED && c.mixed_step_limit == BH_STEP_LIMIT_NONE;
+    F.hmax_a = capped ? kHmaxA : (none ? 1e30 : kHmaxLoose);
+    F.hmax_b = capped ? kHmaxB : (none ? 1e30 : 0.0);
+    // The final state of an escaping ray is the end of the step that crosses
+    // r_escape (render.cpp:247-251); under the reference's cap that end lies
+    // within hmax(r_escape) beyond it.  An uncapped step may end far beyond,
+    // where a ray from a camera close to the hole has bent further, so the
+    // mixed path shortens a step from inside r_escape that would end beyond
+    // r_escape + hmax(r_escape) to end near r_escape + hmax(r_escape) / 2.
+    const double hm_escape = kHmaxA * maxd(1.0, c.r_escape - F.r_h) + kHmaxB;
+    F.land_escape = (c.precision == BH_PRECISION_MIXED && !capped) ? 1 : 0;
+    F.land_limit = c.r_escape + hm_escape;
+    F.land_target = c.r_escape + 0.5 * hm_escape;
     if (c.mixed_capture != BH_CAPTURE_AUTO && c.mixed_capture != BH_CAPTURE_REFERENCE) {
         err = "unknown mixed_capture";
         return BH_ERR_INVALID_ARG;
@@ -524,6 +546,7 @@ FrameParams binary64_treatment(const FrameParams& F) {
     G.atol = F.atol_ref;
     G.hmax_a = kHmaxA;
     G.hmax_b = kHmaxB;
+    G.land_escape = 0;
     G.early_capture = 0;
     G.mirror_ok = 0;
     return G;

@@ -182,11 +182,13 @@ __device__ __forceinline__ void shift_sincos(double s0, double c0, double d, dou
 
 // ---- packed binary32 pairs ----------------------------------------------------
 // sm_100's f32x2 arithmetic: one instruction does the same binary32 operation,
-// rounded to nearest, on the two halves of a 64-bit register pair.  The mixed
-// kernel pairs independent operations of one ray: in the right-hand side,
-// and in the stage sums, which run on the six components as three pairs in
-// the order and with the roundings of the scalar form (product, then fused
-// multiply-adds, then the fused y + h * sum).
+// rounded to nearest, on the two halves of a 64-bit register pair.  The stage
+// sums of the mixed kernel run on the six components as three pairs, in the
+// order and with the roundings of the scalar form (product, then fused
+// multiply-adds, then the fused y + h * sum).  (Pairing the independent
+// products of the right-hand side the same way was measured slower: 4.10
+// against 3.98 ms on the 1024^2 edge-on frame, the pairs' register moves and
+// spills outweighing the instructions saved.)
 using u64 = unsigned long long;
 __device__ __forceinline__ u64 pk2(float lo, float hi) {
     u64 r;
@@ -206,11 +208,6 @@ __device__ __forceinline__ u64 mul2(u64 a, u64 b) {
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
 }
-__device__ __forceinline__ u64 sub2(u64 a, u64 b) {
-    u64 d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
 
 // Hamilton's equations for H = 1/2 g^{mu nu} p_mu p_nu (geodesic.h:50-71),
 // with the Kerr inverse metric in Carter's separated form
@@ -222,72 +219,11 @@ __device__ __forceinline__ u64 sub2(u64 a, u64 b) {
 // not imposed (B is the full bracket).  Delta = (r - r_+)(r - r_-) with each
 // factor formed against a two-term r_+-, so the factor that vanishes at the
 // horizon is exact.  sn, cs: sin and cos of th.
-//
-// The binary32 form pairs the independent products and sums in f32x2
-// instructions (the same operations, grouped two by two; d4 and d5 with their
-// terms gathered as -iS/2 (Dr (p_r^2 + KiD^2) - 2 r (2 E KiD + B iS)) and
-// -sin cos iS (a^2 E^2 - L_z^2 isn2^2 + a^2 B iS)).
-__device__ __forceinline__ void rhs_sc_x2(const Lane<Mixed>& L, float r, float sn, float cs, float pr, float pth,
-                                          float* d, Aux<Mixed>* aux) {
-    if (fabsf(sn) < 1e-9f) sn = (sn < 0.f) ? -1e-9f : 1e-9f;        // kerr.h:51
-    float sn2, cs2;
-    up2(mul2(pk2(sn, cs), pk2(sn, cs)), sn2, cs2);
-    const float r2 = r * r;
-    const float S = fmaf(L.a2R, cs2, r2);
-    float D;
-    if (L.factored) {
-        float f1, f2;
-        up2(sub2(sub2(pk2(r, r), pk2(L.rp_hi, L.rm_hi)), pk2(L.rp_lo, L.rm_lo)), f1, f2);
-        D = f1 * f2;
-    } else {
-        D = r2 - 2.f * r + L.a2R;
-    }
-    const float SD = S * D;
-    const float inv = Mixed::rcp(SD * sn2);
-    float iS, iD;
-    up2(mul2(mul2(pk2(D, S), pk2(sn2, sn2)), pk2(inv, inv)), iS, iD);
-    const float isn2 = inv * SD;
-    const float r2a2 = r2 + L.a2R;
-    float K, Lp;                                       // (r^2+a^2) E - a L_z, L_z - a E sin^2
-    up2(fma2(pk2(r2a2, -L.aE), pk2(L.E, sn2), pk2(-L.aLz, L.Lz)), K, Lp);
-    const float KiD = K * iD;
-    float Dpr, Lpi;                                    // Delta p_r, Lp isn2
-    up2(mul2(pk2(D, Lp), pk2(pr, isn2)), Dpr, Lpi);
-    float m1, m2;                                      // p_th^2, -K KiD
-    up2(mul2(pk2(pth, -K), pk2(pth, KiD)), m1, m2);
-    float b1, b2;
-    up2(fma2(pk2(Dpr, Lpi), pk2(pr, Lp), pk2(m1, m2)), b1, b2);
-    const float B = b1 + b2;
-    float u0, u3;
-    up2(fma2(pk2(r2a2, L.aR), pk2(KiD, KiD), pk2(L.aR * Lp, Lpi)), u0, u3);
-    up2(mul2(pk2(u0, u3), pk2(iS, iS)), d[0], d[3]);
-    up2(mul2(pk2(Dpr, pth), pk2(iS, iS)), d[1], d[2]);
-    const float BiS = B * iS;
-    float p2, k2;
-    up2(mul2(pk2(pr, KiD), pk2(pr, KiD)), p2, k2);
-    const float Dr = fmaf(2.f, r, -2.f);
-    const float Q = fmaf(2.f * L.E, KiD, BiS);
-    const float in4 = fmaf(Dr, p2 + k2, -2.f * r * Q);
-    const float in5 = fmaf(L.a2R, BiS, fmaf(-L.Lz2, isn2 * isn2, L.a2E2));
-    up2(mul2(pk2(-0.5f * iS, -(sn * cs) * iS), pk2(in4, in5)), d[4], d[5]);
-    if (aux) {
-        aux->sn = sn;
-        aux->cs = cs;
-        aux->sn2 = sn2;
-        aux->cs2 = cs2;
-        aux->D = D;
-    }
-}
-
 template <class P>
 __device__ __forceinline__ void rhs_sc(const Lane<P>& L, typename P::R r, typename P::R sn,
                                        typename P::R cs, typename P::R pr, typename P::R pth,
                                        typename P::R* d, Aux<P>* aux) {
     using R = typename P::R;
-    if constexpr (P::kMixed) {
-        rhs_sc_x2(L, r, sn, cs, pr, pth, d, aux);
-        return;
-    }
     if (fabs(sn) < R(1e-9)) sn = (sn < R(0)) ? R(-1e-9) : R(1e-9);   // kerr.h:51
     const R sn2 = sn * sn, cs2 = cs * cs;
     const R r2 = r * r;
@@ -632,6 +568,14 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         L.c0 = ax.cs;
         L.sn0 = ax.sn;
         L.have_k1 = 1;
+    }
+    if (L.tries == 0 && F.land_escape && L.k1[1] > typename P::R(0) &&
+        (float)L.y[1] + (float)L.h * (float)L.k1[1] > (float)F.land_limit && (double)L.y[1] < F.r_escape) {
+        // An escaping step lands within the reference's cap of r_escape: a
+        // step predicted (to first order) to end beyond land_limit ends near
+        // land_target instead, as it would under the reference's step cap.
+        const double hl = (F.land_target - (double)L.y[1]) / (double)L.k1[1];
+        if (hl > 0.0 && hl < L.h) L.h = hl;
     }
     const R h = (R)L.h;
     R t[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], yn[6];

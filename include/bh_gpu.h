@@ -86,10 +86,13 @@ enum {
    control; the binary64 path always does.
      BH_STEP_LIMIT_AUTO       the reference cap when the Sun, a neutron star
                               or a jet is in the scene (their hit tests and
-                              the jet's quadrature sample each step), steps
-                              set by the error control alone otherwise;
+                              the jet's quadrature sample each step), a looser
+                              cap h <= 0.3 max(1, r - r_+) otherwise;
      BH_STEP_LIMIT_REFERENCE  the reference cap;
-     BH_STEP_LIMIT_NONE       steps set by the error control alone. */
+     BH_STEP_LIMIT_NONE       steps set by the error control alone.
+   Without the reference cap, a step that leaves the escape sphere is
+   shortened to end within the reference cap's step of r_escape, where the
+   reference's last step ends. */
 enum { BH_STEP_LIMIT_AUTO = 0, BH_STEP_LIMIT_REFERENCE = 1, BH_STEP_LIMIT_NONE = 2 };
 
 /* How the MIXED path ends a ray that moves inwards inside the innermost

@@ -8,11 +8,15 @@ Tolerances.  The FP64 path evaluates the same Hamiltonian system as the
 reference in a different but algebraically identical form, with CUDA's libm
 and FMA contraction, so results agree to rounding except where a rounding
 difference flips an accept/reject decision or a class (shadow edge, disc
-edge, photon ring).  Hence: class agreement >= 98% and, among rays of equal
-class, the 99th percentile of |g - g_ref|/g_ref, of the sky-direction angle
-and of |Y - Y_ref|/Y_ref below 1e-6.  The mixed path is held to the stated
-accuracy target: 99th percentile of the g error <= 1e-3 and of the direction
-error <= 1e-4 rad, class agreement >= 97%.
+edge, photon ring).  Measured on every golden window: no ray in another
+class, g and direction within 2e-11 (relative, rad), luminance within
+1.2e-6.  Held: at most MAX_CLASS_FLIPS rays of another class per window;
+among rays of equal class every g and direction within FP64_MAX and the
+99th percentiles of g, direction and luminance within 1e-6, medians within
+1e-9.  The mixed path is held to the stated accuracy target on every ray
+of equal class: g within 1e-3, direction within 1e-4 rad, the jet integral
+within 1e-3 (measured maxima 2.4e-5, 1.3e-5 rad, 2.5e-4), with the same
+bound on class flips.
 """
 import math
 import os
@@ -33,8 +37,11 @@ from blackhole_b200 import BHError, RenderConfig, RenderStats, abi  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-6
+FP64_MAX = 1e-7
 MIXED_G_TOL = 1e-3
 MIXED_DIR_TOL = 1e-4
+# Rays of another class than the checker's, at most, per golden window.
+MAX_CLASS_FLIPS = 2
 
 
 def _golden(name):
@@ -56,13 +63,16 @@ def test_fp64_matches_reference_golden(renderer, name):
     s = compare(gw, _golden(name))
     msg = summary(s)
     print(name, msg)
-    assert s["class_agree"] >= 0.98, msg
-    assert s["jet_missing"] <= 0.01 * s["n"], msg
+    assert round((1 - s["class_agree"]) * s["n"]) <= MAX_CLASS_FLIPS, msg
+    assert s["jet_missing"] <= MAX_CLASS_FLIPS, msg
     for k in ("g_rel", "dir_rad", "Y_rel", "jet_rel"):
         assert q(s[k], 0.99) <= FP64_TOL, f"{k}: {msg}"
         # most rays reproduce the reference to rounding
         if len(s[k]) >= 20:
             assert q(s[k], 0.5) <= 1e-9, f"{k}: {msg}"
+    for k in ("g_rel", "dir_rad"):
+        if len(s[k]):
+            assert s[k].max() <= FP64_MAX, f"{k}: {msg}"
 
 
 @pytest.mark.parametrize("name", ["a09_i60_centre", "a09_i60_corner", "a0998_i85_ring", "quasar_jets", "m87_jets"])
@@ -74,15 +84,12 @@ def test_mixed_meets_accuracy_target_against_reference(renderer, name):
     s = compare(gw, _golden(name))
     msg = summary(s)
     print(name, "mixed", msg)
-    assert s["class_agree"] >= 0.97, msg
-    # at least 99% of the rays within the target (all of them when fewer
-    # than 100 rays of the kind are in the window)
+    assert round((1 - s["class_agree"]) * s["n"]) <= MAX_CLASS_FLIPS, msg
+    # every ray of equal class within the target
     for k, tol in (("g_rel", MIXED_G_TOL), ("dir_rad", MIXED_DIR_TOL), ("jet_rel", MIXED_G_TOL)):
         v = s[k]
-        if len(v) >= 100:
-            assert (v <= tol).mean() >= 0.99, msg
-        elif len(v):
-            assert v.max() <= 10 * tol, msg
+        if len(v):
+            assert v.max() <= tol, f"{k}: {msg}"
 
 
 def test_fp64_frame_pixels_match_reference_render(renderer):

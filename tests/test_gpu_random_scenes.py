@@ -2,7 +2,17 @@
 pinned bit for bit to the reference) and the mixed path against the FP64 GPU
 path, over spins, inclinations, camera distances, fields of view, disc
 extents, senses, samples per pixel, sky and stop rules chosen at random.
-Each scene is a small window, so the oracle finishes in seconds."""
+Each scene is a small window, so the oracle finishes in seconds.
+
+Held: the FP64 path within 1e-6 (95th percentile) of the oracle with at most
+two rays of another class; the mixed path with at most two rays of another
+class than the FP64 path's and every ray of equal class within the target
+(g 1e-3, direction 1e-4 rad), except rays whose FP64 result moves by more
+than 1e-5 when the camera turns by 1.5e-10 rad (the conditioning probe of
+the benchmark-frame tests; at most 0.5% of a scene's rays).  Measured over
+the twelve scenes: no class flips, mixed g within 1.7e-5, direction within
+1.0e-4 rad."""
+import copy
 import math
 import os
 import sys
@@ -12,6 +22,7 @@ import pytest
 
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 from parity import compare, q, summary  # noqa: E402
+from test_gpu_headline_strip import _moved  # noqa: E402
 
 from blackhole_b200 import abi  # noqa: E402
 from blackhole_b200.config import M_SUN, Camera, RenderConfig  # noqa: E402
@@ -48,14 +59,23 @@ def test_random_scene_fp64_matches_oracle_and_mixed_meets_target(renderer, orc, 
     g64 = renderer.trace_rays(cfg)
     s = compare(g64, chk)
     msg = f"seed {seed}: {summary(s)}"
-    assert s["class_agree"] >= 0.97, msg
+    assert (g64["what"] != chk["what"]).sum() <= 2, msg
     for k in ("g_rel", "dir_rad", "Y_rel"):
         assert q(s[k], 0.95) <= 1e-6, msg
+    turned = copy.deepcopy(cfg)
+    turned.cam.yaw += 1.5e-10
+    moved = _moved(g64, renderer.trace_rays(turned))
     cfg.precision = abi.PRECISION_MIXED
     gm = renderer.trace_rays(cfg)
     sm = compare(gm, g64)
     msg = f"seed {seed} mixed: {summary(sm)}"
-    assert sm["class_agree"] >= 0.95, msg
-    for k, tol in (("g_rel", 1e-3), ("dir_rad", 1e-4)):
-        if len(sm[k]):
-            assert (sm[k] <= tol).mean() >= 0.97, msg
+    same = gm["what"] == g64["what"]
+    assert (~same).sum() <= 2, msg
+    well = moved <= 1e-5
+    assert (~well & same & ((g64["what"] == abi.HIT_DISC) | (g64["what"] == abi.HIT_SKY))).mean() <= 0.005, msg
+    disc = same & well & (g64["what"] == abi.HIT_DISC) & (g64["g"] > 0)
+    g_err = np.abs(gm["g"] - g64["g"]) / np.where(g64["g"] > 0, g64["g"], 1.0)
+    assert not (disc & (g_err > 1e-3)).any(), (g_err[disc].max(), msg)
+    sky = same & well & (g64["what"] == abi.HIT_SKY)
+    ang = 2.0 * np.arcsin(np.clip(np.linalg.norm(gm["dir"] - g64["dir"], axis=1) / 2.0, 0.0, 1.0))
+    assert not (sky & (ang > 1e-4)).any(), (ang[sky].max(), msg)
