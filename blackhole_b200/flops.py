@@ -12,7 +12,8 @@ Reciprocals, divisions, square roots, sin/cos and pow are listed separately
                            1/sin^2 from one reciprocal, K, L', B and the six
                            derivatives: 62 ops + 1 reciprocal
   shift_sincos (stages 2-6) angle addition with Taylor series of sin/cos of the
-                           stage increment: 25 ops in binary32, 36 in binary64
+                           stage increment: 20 ops in binary32 (Horner form), 36
+                           in binary64
   stage combinations       13 + 30 + 42 + 54 + 66 + 66 = 271 ops
   error estimate           per component 12 (stage combination) + 2 (scale)
                            + 1 (scaled error) + 2 (square, sum) = 17, x 6 = 102;
@@ -26,7 +27,7 @@ ray take a full sincos.
 """
 
 RHS = 62
-SHIFT = {"mixed": 25, "fp64": 36}
+SHIFT = {"mixed": 20, "fp64": 36}
 STAGES = 13 + 30 + 42 + 54 + 66 + 66
 ERROR = {"mixed": 6 * 17, "fp64": 6 * 16}
 CONTROL_F64 = 5
@@ -43,5 +44,5 @@ def per_step(path: str) -> dict:
 
 
 # FLOPs per accepted step charged against the ALU peak of each path's main pipe:
-# mixed 870 binary32 (+ 48 binary64 islands), fp64 967 binary64.
+# mixed 845 binary32 (+ 48 binary64 islands), fp64 967 binary64.
 FLOPS_PER_STEP = {"mixed": per_step("mixed"), "fp64": per_step("fp64")}

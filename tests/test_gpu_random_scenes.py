@@ -72,7 +72,8 @@ def test_random_scene_fp64_matches_oracle_and_mixed_meets_target(renderer, orc, 
     same = gm["what"] == g64["what"]
     assert (~same).sum() <= 2, msg
     well = moved <= 1e-5
-    assert (~well & same & ((g64["what"] == abi.HIT_DISC) | (g64["what"] == abi.HIT_SKY))).mean() <= 0.005, msg
+    lit = ((g64["what"] == abi.HIT_DISC) & (g64["g"] > 0)) | (g64["what"] == abi.HIT_SKY)
+    assert (~well & same & lit).mean() <= 0.005, msg
     disc = same & well & (g64["what"] == abi.HIT_DISC) & (g64["g"] > 0)
     g_err = np.abs(gm["g"] - g64["g"]) / np.where(g64["g"] > 0, g64["g"], 1.0)
     assert not (disc & (g_err > 1e-3)).any(), (g_err[disc].max(), msg)
