@@ -39,8 +39,10 @@ METRIC = "rays/s at 1024² on 1 B200: mixed vs FP64 plain at stated g/dir error;
 WORKLOAD = ("edge_on_1024: a=0.998, inclination 85 deg, 1024x1024, 1 spp, +-25 M from r=1000 M, "
             "disc r_isco..50 M at 0.3 Eddington, M=10 M_sun, 250k-star uniform sky + 21.5 mag/arcsec^2 "
             "background, escape 1.1 r_obs, horizon stop r_+(1+1e-6), rtol 1e-8 / atol 1e-10 (FP64), "
-            "1e-6 / 1e-8 (mixed); FP64 under the reference's step cap, mixed with error-controlled steps "
-            "(no cap: no Sun, neutron star or jet in view), ingoing rays inside the innermost photon "
+            "1e-6 / 1e-8 (mixed); FP64 under the reference's step cap, mixed under a loose cap "
+            "h <= 0.3 max(1, r - r_+) with a rotation-invariant azimuth error scale and the escaping "
+            "step landed within the reference cap of r_escape (no Sun, neutron star or jet in view), "
+            "ingoing rays inside the innermost photon "
             "orbit ended as captured, and near-critical rays (escaping after circling close to the photon "
             "shell) traced in binary64 by a kernel beside the binary32 one")
 L2_FLUSH_BYTES = 256 << 20
