@@ -50,6 +50,9 @@ struct bh_ctx {
     unsigned long long budget = 0;
     std::atomic<int> abort_requested{0};
     int32_t* h_one = nullptr;          // pinned 1, source of the abort copy
+    // Pinned read-back of a single-frame launch's queue state and stats,
+    // copied on the stream before the call's one synchronisation.
+    unsigned char* h_readback = nullptr;
 
     std::vector<double> h_table;
     double* d_table = nullptr;
@@ -415,13 +418,31 @@ int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_
     return record_launch(ctx, p, stream, timed);
 }
 
-// Read back the queue state and per-frame stats after the stream drained.
+constexpr size_t kReadbackBytes = sizeof(QueueState) + sizeof(FrameStats);
+
+// Enqueue the copies of a single-frame launch's queue state and stats into
+// the pinned read-back buffer (read by finish(..., prefetched = true) once
+// the stream has drained), so the call synchronises once.
+int enqueue_readback(bh_ctx* ctx, cudaStream_t stream) {
+    CK(cudaMemcpyAsync(ctx->h_readback, ctx->d_queue, sizeof(QueueState), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(ctx->h_readback + sizeof(QueueState), ctx->fstats.p, sizeof(FrameStats),
+                       cudaMemcpyDeviceToHost, stream));
+    return BH_OK;
+}
+
+// Read back the queue state and per-frame stats after the stream drained
+// (from the read-back buffer when enqueue_readback filled it).
 int finish(bh_ctx* ctx, int n, bh_render_stats* per_frame, bh_render_stats* total, bool timed,
-           double seconds) {
+           double seconds, bool prefetched = false) {
     QueueState q;
-    CK(cudaMemcpy(&q, ctx->d_queue, sizeof q, cudaMemcpyDeviceToHost));
     std::vector<FrameStats> fs(n);
-    CK(cudaMemcpy(fs.data(), ctx->fstats.p, n * sizeof(FrameStats), cudaMemcpyDeviceToHost));
+    if (prefetched && n == 1) {
+        std::memcpy(&q, ctx->h_readback, sizeof q);
+        std::memcpy(fs.data(), ctx->h_readback + sizeof(QueueState), sizeof(FrameStats));
+    } else {
+        CK(cudaMemcpy(&q, ctx->d_queue, sizeof q, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(fs.data(), ctx->fstats.p, n * sizeof(FrameStats), cudaMemcpyDeviceToHost));
+    }
     ctx->d2h += static_cast<long long>(sizeof q + n * sizeof(FrameStats));
     float t_trace = 0.f, t_shade = 0.f;
     if (timed) {
@@ -517,6 +538,9 @@ int bh_gpu_create(int device, bh_ctx** out) {
     if ((e = cudaMemset(ctx->d_queue, 0, sizeof(QueueState))) != cudaSuccess) return bail(e);
     if ((e = cudaHostAlloc(&ctx->h_one, sizeof(int32_t), cudaHostAllocDefault)) != cudaSuccess) return bail(e);
     *ctx->h_one = 1;
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_readback), kReadbackBytes, cudaHostAllocDefault)) !=
+        cudaSuccess)
+        return bail(e);
     for (auto& ev : ctx->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreateWithFlags(&ctx->stage_free, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
@@ -541,6 +565,7 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     cudaFree(ctx->d_bin_start);
     cudaFree(ctx->d_queue);
     if (ctx->h_one) cudaFreeHost(ctx->h_one);
+    if (ctx->h_readback) cudaFreeHost(ctx->h_readback);
     if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
     if (ctx->stage) cudaFreeHost(ctx->stage);
     if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
@@ -570,11 +595,12 @@ int bh_gpu_render(bh_ctx* ctx, const bh_render_config* cfg, bh_xyz* out_pixels, 
     if (rc != BH_OK) return rc;
     CK(cudaMemcpyAsync(out_pixels, ctx->pixels.p, npx * sizeof(bh_xyz), cudaMemcpyDeviceToHost, ctx->stream));
     ctx->d2h += static_cast<long long>(npx * sizeof(bh_xyz));
+    if ((rc = enqueue_readback(ctx, ctx->stream)) != BH_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     bh_render_stats local;
     std::memset(&local, 0, sizeof local);
-    rc = finish(ctx, 1, nullptr, &local, true, secs);
+    rc = finish(ctx, 1, nullptr, &local, true, secs, true);
     if (stats) {
         bh_render_stats s = local;
         stats->rays += s.rays; stats->steps += s.steps; stats->captured += s.captured;
@@ -606,9 +632,10 @@ int bh_gpu_render_device(bh_ctx* ctx, const bh_render_config* cfg, bh_xyz* d_pix
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
     rc = enqueue(ctx, frames, d_pixels, nullptr, s, stats != nullptr);
     if (rc != BH_OK || !stats) return rc;
+    if ((rc = enqueue_readback(ctx, s)) != BH_OK) return rc;
     CK(cudaStreamSynchronize(s));
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    return finish(ctx, 1, stats, nullptr, true, secs);
+    return finish(ctx, 1, stats, nullptr, true, secs, true);
 }
 
 int bh_gpu_trace_rays(bh_ctx* ctx, const bh_render_config* cfg, bh_ray_result* out, bh_render_stats* stats) {
@@ -628,9 +655,10 @@ int bh_gpu_trace_rays(bh_ctx* ctx, const bh_render_config* cfg, bh_ray_result* o
     if (rc != BH_OK) return rc;
     CK(cudaMemcpyAsync(out, ctx->rays.p, nr * sizeof(bh_ray_result), cudaMemcpyDeviceToHost, ctx->stream));
     ctx->d2h += static_cast<long long>(nr * sizeof(bh_ray_result));
+    if ((rc = enqueue_readback(ctx, ctx->stream)) != BH_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    return finish(ctx, 1, stats, nullptr, true, secs);
+    return finish(ctx, 1, stats, nullptr, true, secs, true);
 }
 
 int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz* const* outs,
