@@ -5,6 +5,7 @@
 // sky mode change), and grow-only ray/pixel buffers.  A render call is: frame
 // constants -> H2D, queue reset, the persistent trace kernel, the shade
 // kernel, the stats reduction, D2H of pixels and stats.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,6 +54,13 @@ struct bh_ctx {
     // Pinned read-back of a single-frame launch's queue state and stats,
     // copied on the stream before the call's one synchronisation.
     unsigned char* h_readback = nullptr;
+    // bh_gpu_render's row-band pipeline: the driver's stream wait on a device
+    // word (null where the driver does not offer it: no pipeline), the
+    // highest-priority stream the bands are shaded and copied on, the event
+    // that joins it back, and the per-band finished-ray counters.
+    CUresult (*wait_value32)(CUstream, CUdeviceptr, cuuint32_t, unsigned int) = nullptr;
+    cudaStream_t band_stream = nullptr;
+    cudaEvent_t band_join = nullptr;
 
     std::vector<double> h_table;
     double* d_table = nullptr;
@@ -71,6 +79,7 @@ struct bh_ctx {
     // Adjoint: target image, per-ray gradients and luminances, checkpoint
     // slots, counters, sums and the edge pass's buffers.
     DevBuf adj_target, adj_grad, adj_Y, adj_ckpt, adj_counters, adj_sums, adj_xr, adj_cand, adj_edge, adj_high;
+    DevBuf band_done;
     // Display transform: blur scratch, glare weights, meter state, 8-bit output.
     DevBuf disp_tmp, disp_near, disp_far, disp_k, disp_state, disp_rgb;
     // bh_gpu_eval: inputs and outputs.
@@ -409,6 +418,97 @@ int record_launch(bh_ctx* ctx, const Plan& p, cudaStream_t stream, bool timed, b
     return BH_OK;
 }
 
+// ---- bh_gpu_render's row-band pipeline -------------------------------------
+// The frame's rays are handed out in pixel order, so its rows finish roughly
+// in order while the trace runs.  The trace kernels count each band's
+// finished rays; a highest-priority stream waits (in the GPU's front end, not
+// on an SM) for each band's count, shades that band and copies its rows to
+// the host while the rest of the frame is still being traced.  The binary32
+// trace grid gives up kBandReserveBlocks block slots so the band shading has
+// room on the SMs while the trace runs.
+constexpr int kBandRows = 64;              // rows per band (a multiple of the 4-row pixel order)
+constexpr int kBandReserveBlocks = 0;
+
+void setup_band_pipeline(bh_ctx* ctx) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuStreamWaitValue32", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        cudaGetLastError();
+        return;
+    }
+    int lo = 0, hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->band_stream, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->band_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    // The wait must work here: one on a word this stream has just zeroed
+    // (the queue's first counter, zero anyway) returns at once.
+    auto wait = reinterpret_cast<CUresult (*)(CUstream, CUdeviceptr, cuuint32_t, unsigned int)>(fn);
+    if (cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int), ctx->band_stream) != cudaSuccess ||
+        wait(ctx->band_stream, reinterpret_cast<CUdeviceptr>(ctx->d_queue), 0u, CU_STREAM_WAIT_VALUE_GEQ) !=
+            CUDA_SUCCESS ||
+        cudaStreamSynchronize(ctx->band_stream) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    ctx->wait_value32 = wait;
+}
+
+// The launch of plan `p` (one frame, d_pixels on the device) with its rows
+// shaded and copied to `out_pixels` band by band as they finish.
+int record_banded(bh_ctx* ctx, Plan& p, const bh_render_config* cfg, bh_xyz* out_pixels, cudaStream_t stream) {
+    const int W = cfg->width, H = cfg->height;
+    const int S = cfg->sqrt_spp > 1 ? cfg->sqrt_spp : 1;
+    const int nb = (H + kBandRows - 1) / kBandRows;
+    const long long px_band = static_cast<long long>(kBandRows) * W;
+    int rc;
+    if ((rc = ensure(ctx, ctx->band_done, static_cast<size_t>(nb) * sizeof(unsigned int))) != BH_OK) return rc;
+    unsigned int* done = static_cast<unsigned int*>(ctx->band_done.p);
+    p.tl.band_done = done;
+    p.tl.rays_per_band = px_band * S * S;
+    p.tl.nbands = nb;
+    if (kBandReserveBlocks > 0 && p.tl.grid > 2 * kBandReserveBlocks) p.tl.grid -= kBandReserveBlocks;
+    const unsigned char* st = ctx->stage;
+    const size_t fbytes = static_cast<size_t>(p.nf) * sizeof(FrameParams);
+    CK(cudaMemcpyAsync(ctx->frames.p, st, fbytes, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->ray_end.p, st + fbytes, sizeof(long long), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(ctx->pix_end.p, st + fbytes + sizeof(long long), sizeof(long long), cudaMemcpyHostToDevice,
+                       stream));
+    CK(cudaMemcpyAsync(ctx->d_queue, st + fbytes + 2 * sizeof(long long), sizeof(QueueState), cudaMemcpyHostToDevice,
+                       stream));
+    CK(cudaEventRecord(ctx->stage_free, stream));
+    CK(cudaMemsetAsync(done, 0, static_cast<size_t>(nb) * sizeof(unsigned int), stream));
+    CK(cudaEventRecord(ctx->ev[0], stream));
+    // The band stream starts once the counters are cleared.
+    CK(cudaStreamWaitEvent(ctx->band_stream, ctx->ev[0], 0));
+    if (p.rays > 0) CK(launch_trace(p.tl, stream));
+    CK(cudaEventRecord(ctx->ev[1], stream));
+    const long long npx = static_cast<long long>(W) * H;
+    for (int b = 0; b < nb; ++b) {
+        const long long lo = b * px_band;
+        const long long hi = std::min(npx, lo + px_band);
+        const long long rays = (hi - lo) * S * S;
+        if (ctx->wait_value32(ctx->band_stream, reinterpret_cast<CUdeviceptr>(done + b),
+                              static_cast<cuuint32_t>(rays), CU_STREAM_WAIT_VALUE_GEQ) != CUDA_SUCCESS)
+            return fail(ctx, BH_ERR_CUDA, "stream wait on a row band failed");
+        ShadeLaunch sl = p.sl;
+        sl.pixel_lo = lo;
+        sl.total_pixels = hi;
+        CK(launch_shade(sl, ctx->band_stream));
+        CK(cudaMemcpyAsync(out_pixels + lo, static_cast<bh_xyz*>(ctx->pixels.p) + lo,
+                           static_cast<size_t>(hi - lo) * sizeof(bh_xyz), cudaMemcpyDeviceToHost, ctx->band_stream));
+    }
+    CK(cudaEventRecord(ctx->band_join, ctx->band_stream));
+    CK(cudaStreamWaitEvent(stream, ctx->band_join, 0));
+    CK(cudaEventRecord(ctx->ev[2], stream));
+    CK(launch_reduce(p.rl, stream));
+    ctx->d2h += npx * static_cast<long long>(sizeof(bh_xyz));
+    return BH_OK;
+}
+
 int enqueue(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels, bh_ray_result* d_rays,
             cudaStream_t stream, bool timed) {
     Plan p;
@@ -541,6 +641,7 @@ int bh_gpu_create(int device, bh_ctx** out) {
     if ((e = cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_readback), kReadbackBytes, cudaHostAllocDefault)) !=
         cudaSuccess)
         return bail(e);
+    setup_band_pipeline(ctx);
     for (auto& ev : ctx->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreateWithFlags(&ctx->stage_free, cudaEventDisableTiming)) != cudaSuccess) return bail(e);
@@ -557,7 +658,7 @@ void bh_gpu_destroy(bh_ctx* ctx) {
                       &ctx->adj_ckpt, &ctx->adj_counters, &ctx->adj_sums, &ctx->adj_xr, &ctx->adj_cand, &ctx->adj_edge,
                       &ctx->adj_high, &ctx->eval_in, &ctx->eval_out, &ctx->disp_tmp, &ctx->disp_near,
                       &ctx->disp_far, &ctx->disp_k, &ctx->disp_state, &ctx->disp_rgb, &ctx->sel_flag,
-                      &ctx->sel_list})
+                      &ctx->sel_list, &ctx->band_done})
         if (b->p) cudaFree(b->p);
     cudaFree(ctx->d_table);
     cudaFree(ctx->d_star_pos);
@@ -566,6 +667,8 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     cudaFree(ctx->d_queue);
     if (ctx->h_one) cudaFreeHost(ctx->h_one);
     if (ctx->h_readback) cudaFreeHost(ctx->h_readback);
+    if (ctx->band_stream) cudaStreamDestroy(ctx->band_stream);
+    if (ctx->band_join) cudaEventDestroy(ctx->band_join);
     if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
     if (ctx->stage) cudaFreeHost(ctx->stage);
     if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);
@@ -591,10 +694,19 @@ int bh_gpu_render(bh_ctx* ctx, const bh_render_config* cfg, bh_xyz* out_pixels, 
     if (rc != BH_OK) return rc;
     const size_t npx = static_cast<size_t>(cfg->width) * cfg->height;
     if ((rc = ensure(ctx, ctx->pixels, npx * sizeof(bh_xyz))) != BH_OK) return rc;
-    rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true);
-    if (rc != BH_OK) return rc;
-    CK(cudaMemcpyAsync(out_pixels, ctx->pixels.p, npx * sizeof(bh_xyz), cudaMemcpyDeviceToHost, ctx->stream));
-    ctx->d2h += static_cast<long long>(npx * sizeof(bh_xyz));
+    if (ctx->wait_value32 && cfg->height >= 2 * kBandRows) {
+        // rows shaded and copied out band by band while the frame is traced
+        Plan p;
+        if ((rc = plan_launch(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, true, p)) != BH_OK)
+            return rc;
+        ctx->h2d += static_cast<long long>(p.stage_bytes);
+        if ((rc = record_banded(ctx, p, cfg, out_pixels, ctx->stream)) != BH_OK) return rc;
+    } else {
+        rc = enqueue(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, ctx->stream, true);
+        if (rc != BH_OK) return rc;
+        CK(cudaMemcpyAsync(out_pixels, ctx->pixels.p, npx * sizeof(bh_xyz), cudaMemcpyDeviceToHost, ctx->stream));
+        ctx->d2h += static_cast<long long>(npx * sizeof(bh_xyz));
+    }
     if ((rc = enqueue_readback(ctx, ctx->stream)) != BH_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -50,6 +50,14 @@ struct TraceLaunch {
     int* sel_list;                   // device, total_rays: the near-critical rays' ids
     cudaStream_t side_stream;
     cudaEvent_t fork_event, join_event;
+    // Row bands of a single-frame launch whose pixels are shaded and copied
+    // out while the rest of the frame is traced: each finished ray adds one
+    // to band_done[gid / rays_per_band]; after the last trace kernel every
+    // counter is raised to its band's size (so a wait on it always ends).
+    // Null: no counting.
+    unsigned int* band_done;
+    long long rays_per_band;
+    int nbands;
 };
 
 // Bytes of one deferred-ray record.
@@ -78,6 +86,7 @@ struct ShadeLaunch {
     double* pixel_lum;               // device, total_pixels luminance for the flux sum
     unsigned char* ray_class;        // device, per-ray class after shading
     const double* jet;               // jet emission per ray (TraceLaunch::jet), or null
+    long long pixel_lo;              // shade global pixels [pixel_lo, total_pixels) only
 };
 
 cudaError_t launch_shade(const ShadeLaunch& L, cudaStream_t stream);

@@ -295,10 +295,11 @@ struct ShadeArgs {
     bh_ray_result* rays;
     double* pixel_lum;
     const double* jet;
+    long long pixel_lo;
 };
 
 __global__ void shade_kernel(ShadeArgs A) {
-    const long long gp = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long gp = A.pixel_lo + (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gp >= A.total_pixels) return;
     const int f = find_frame(A.frame_pixel_end, A.nframes, gp);
     const FrameParams& F = A.frames[f];
@@ -497,8 +498,10 @@ cudaError_t launch_shade(const ShadeLaunch& L, cudaStream_t stream) {
     A.rays = L.rays;
     A.pixel_lum = L.pixel_lum;
     A.jet = L.jet;
+    A.pixel_lo = L.pixel_lo;
     const int bs = 128;
-    const long long grid = (L.total_pixels + bs - 1) / bs;
+    const long long grid = (L.total_pixels - L.pixel_lo + bs - 1) / bs;
+    if (grid <= 0) return cudaSuccess;
     shade_kernel<<<(unsigned)grid, bs, 0, stream>>>(A);
     return cudaGetLastError();
 }

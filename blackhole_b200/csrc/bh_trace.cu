@@ -361,6 +361,8 @@ struct TraceArgs {
     long long list_cap;      // select 1 with a list: the rays [0, list_cap) beside the binary32
                              // kernel (phase 0), the rest [list_cap, ..) after it (phase 1)
     int phase;
+    unsigned int* band_done; // finished rays per row band, or null
+    long long rays_per_band;
 };
 
 template <class P>
@@ -391,6 +393,11 @@ __device__ __forceinline__ void write_hit(const TraceArgs& A, const Lane<P>& L, 
     o->what = what;
     o->steps = L.steps;
     o->attempts = L.attempts;
+    if (A.band_done) {
+        // the record is visible device-wide before its band's count moves
+        __threadfence();
+        atomicAdd(&A.band_done[L.gid / A.rays_per_band], 1u);
+    }
 }
 
 // pi in two binary32 parts: pi - th as (kPiHi - th) + kPiLo, the first
@@ -1112,8 +1119,19 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.budget = L.budget;
     A.jet = L.jet;
     A.xing = L.xing;
+    A.band_done = L.band_done;
+    A.rays_per_band = L.rays_per_band > 0 ? L.rays_per_band : 1;
     trace_kernel<P, MAXREG, JET, SURF><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
+}
+
+// Raises each band counter to its band's ray count (after the trace kernels).
+__global__ void band_release_kernel(unsigned int* band_done, int nbands, long long total, long long per_band) {
+    for (int b = threadIdx.x; b < nbands; b += blockDim.x) {
+        const long long lo = (long long)b * per_band;
+        const long long n = (total - lo < per_band) ? total - lo : per_band;
+        atomicMax(&band_done[b], (unsigned int)(n > 0 ? n : 0));
+    }
 }
 
 // The near-critical test of every ray's initial photon (grid-stride, one
@@ -1234,8 +1252,16 @@ cudaError_t launch_eval_rhs(int precision, const FrameParams* d_frame, const dou
 }
 
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
-    if (L.jet) return launch_trace_t<true, true>(L, stream);
-    return (L.surfaces || L.xing) ? launch_trace_t<false, true>(L, stream) : launch_trace_t<false, false>(L, stream);
+    cudaError_t e;
+    if (L.jet) e = launch_trace_t<true, true>(L, stream);
+    else e = (L.surfaces || L.xing) ? launch_trace_t<false, true>(L, stream) : launch_trace_t<false, false>(L, stream);
+    if (e != cudaSuccess || !L.band_done) return e;
+    // Every band counter up to its band's size once all trace kernels are
+    // done (rays a budget or an abort left untraced included), so a stream
+    // waiting on a band never waits past the trace.
+    band_release_kernel<<<1, 256, 0, stream>>>(L.band_done, L.nbands, L.total_rays,
+                                               L.rays_per_band > 0 ? L.rays_per_band : 1);
+    return cudaGetLastError();
 }
 
 int trace_blocks_per_sm(int precision, int block_size, int variant) {

@@ -372,6 +372,28 @@ def test_device_output_matches_host_output(renderer):
     assert np.array_equal(dev.cpu().numpy(), host)
 
 
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+def test_banded_render_equals_the_device_path(renderer, precision):
+    """bh_gpu_render shades and copies a frame of 128 rows or more band by
+    band while it is traced (rows 64 at a time, each started when the trace
+    has counted all its rays): the same pixels and stats as the device path,
+    which shades the whole frame after the trace; ragged last band."""
+    torch = pytest.importorskip("torch")
+    cfg = kerr_a09_i60(width=200, height=150, sqrt_spp=2, precision=precision)
+    host = np.full((150, 200, 3), np.nan)
+    sh = abi.bh_render_stats()
+    renderer.render_into(cfg, host, sh)
+    dev = torch.empty((150, 200, 3), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    sd = abi.bh_render_stats()
+    renderer.render_device(cfg, dev.data_ptr(), stream.cuda_stream, stats=sd)
+    stream.synchronize()
+    assert np.array_equal(dev.cpu().numpy(), host)
+    for f in ("rays", "steps", "attempts", "captured", "disc_hits", "escaped", "total_flux"):
+        assert getattr(sh, f) == getattr(sd, f), f
+    assert np.array_equal(renderer.render(cfg), host)
+
+
 def test_invariant_diagnostics_of_a_full_frame(renderer):
     """Null-norm and Carter drift stay at the integration tolerance."""
     cfg = kerr_a09_i60(width=128, height=128)
