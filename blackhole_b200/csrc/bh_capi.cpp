@@ -56,11 +56,11 @@ struct bh_ctx {
     unsigned char* h_readback = nullptr;
     // bh_gpu_render's row-band pipeline: the driver's stream wait on a device
     // word (null where the driver does not offer it: no pipeline), the
-    // highest-priority stream the bands are shaded and copied on, the event
-    // that joins it back, and the per-band finished-ray counters.
+    // streams the bands are shaded and copied on, the events that join them
+    // back, and the per-band finished-ray counters.
     CUresult (*wait_value32)(CUstream, CUdeviceptr, cuuint32_t, unsigned int) = nullptr;
-    cudaStream_t band_stream = nullptr;
-    cudaEvent_t band_join = nullptr;
+    cudaStream_t band_stream[8] = {};
+    cudaEvent_t band_join[8] = {};
 
     std::vector<double> h_table;
     double* d_table = nullptr;
@@ -421,13 +421,19 @@ int record_launch(bh_ctx* ctx, const Plan& p, cudaStream_t stream, bool timed, b
 // ---- bh_gpu_render's row-band pipeline -------------------------------------
 // The frame's rays are handed out in pixel order, so its rows finish roughly
 // in order while the trace runs.  The trace kernels count each band's
-// finished rays; a highest-priority stream waits (in the GPU's front end, not
+// finished rays; a stream waits (in the GPU's front end, not
 // on an SM) for each band's count, shades that band and copies its rows to
 // the host while the rest of the frame is still being traced.  The binary32
-// trace grid gives up kBandReserveBlocks block slots so the band shading has
-// room on the SMs while the trace runs.
+// trace grid may give up kBandReserveBlocks block slots for the shading
+// (measured: none is best; the band streams have the trace's priority, a
+// higher one, or slots left free, both slowed the trace more than they
+// gained).  The bands go round kBandStreams
+// streams, so a band whose rays finish late (the photon ring's) holds up only
+// the bands that share its stream.
 constexpr int kBandRows = 64;              // rows per band (a multiple of the 4-row pixel order)
 constexpr int kBandReserveBlocks = 0;
+constexpr int kBandStreams = 8;
+static_assert(kBandStreams <= 8, "bh_ctx holds 8 band streams");
 
 void setup_band_pipeline(bh_ctx* ctx) {
     void* fn = nullptr;
@@ -437,20 +443,19 @@ void setup_band_pipeline(bh_ctx* ctx) {
         cudaGetLastError();
         return;
     }
-    int lo = 0, hi = 0;
-    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->band_stream, cudaStreamNonBlocking, hi) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->band_join, cudaEventDisableTiming) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-    }
+    for (int i = 0; i < kBandStreams; ++i)
+        if (cudaStreamCreateWithFlags(&ctx->band_stream[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->band_join[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
     // The wait must work here: one on a word this stream has just zeroed
     // (the queue's first counter, zero anyway) returns at once.
     auto wait = reinterpret_cast<CUresult (*)(CUstream, CUdeviceptr, cuuint32_t, unsigned int)>(fn);
-    if (cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int), ctx->band_stream) != cudaSuccess ||
-        wait(ctx->band_stream, reinterpret_cast<CUdeviceptr>(ctx->d_queue), 0u, CU_STREAM_WAIT_VALUE_GEQ) !=
+    if (cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int), ctx->band_stream[0]) != cudaSuccess ||
+        wait(ctx->band_stream[0], reinterpret_cast<CUdeviceptr>(ctx->d_queue), 0u, CU_STREAM_WAIT_VALUE_GEQ) !=
             CUDA_SUCCESS ||
-        cudaStreamSynchronize(ctx->band_stream) != cudaSuccess) {
+        cudaStreamSynchronize(ctx->band_stream[0]) != cudaSuccess) {
         cudaGetLastError();
         return;
     }
@@ -482,27 +487,31 @@ int record_banded(bh_ctx* ctx, Plan& p, const bh_render_config* cfg, bh_xyz* out
     CK(cudaEventRecord(ctx->stage_free, stream));
     CK(cudaMemsetAsync(done, 0, static_cast<size_t>(nb) * sizeof(unsigned int), stream));
     CK(cudaEventRecord(ctx->ev[0], stream));
-    // The band stream starts once the counters are cleared.
-    CK(cudaStreamWaitEvent(ctx->band_stream, ctx->ev[0], 0));
+    // The band streams start once the counters are cleared.
+    const int ns = std::min(nb, kBandStreams);
+    for (int i = 0; i < ns; ++i) CK(cudaStreamWaitEvent(ctx->band_stream[i], ctx->ev[0], 0));
     if (p.rays > 0) CK(launch_trace(p.tl, stream));
     CK(cudaEventRecord(ctx->ev[1], stream));
     const long long npx = static_cast<long long>(W) * H;
     for (int b = 0; b < nb; ++b) {
+        cudaStream_t bs = ctx->band_stream[b % ns];
         const long long lo = b * px_band;
         const long long hi = std::min(npx, lo + px_band);
         const long long rays = (hi - lo) * S * S;
-        if (ctx->wait_value32(ctx->band_stream, reinterpret_cast<CUdeviceptr>(done + b),
-                              static_cast<cuuint32_t>(rays), CU_STREAM_WAIT_VALUE_GEQ) != CUDA_SUCCESS)
+        if (ctx->wait_value32(bs, reinterpret_cast<CUdeviceptr>(done + b), static_cast<cuuint32_t>(rays),
+                              CU_STREAM_WAIT_VALUE_GEQ) != CUDA_SUCCESS)
             return fail(ctx, BH_ERR_CUDA, "stream wait on a row band failed");
         ShadeLaunch sl = p.sl;
         sl.pixel_lo = lo;
         sl.total_pixels = hi;
-        CK(launch_shade(sl, ctx->band_stream));
+        CK(launch_shade(sl, bs));
         CK(cudaMemcpyAsync(out_pixels + lo, static_cast<bh_xyz*>(ctx->pixels.p) + lo,
-                           static_cast<size_t>(hi - lo) * sizeof(bh_xyz), cudaMemcpyDeviceToHost, ctx->band_stream));
+                           static_cast<size_t>(hi - lo) * sizeof(bh_xyz), cudaMemcpyDeviceToHost, bs));
     }
-    CK(cudaEventRecord(ctx->band_join, ctx->band_stream));
-    CK(cudaStreamWaitEvent(stream, ctx->band_join, 0));
+    for (int i = 0; i < ns; ++i) {
+        CK(cudaEventRecord(ctx->band_join[i], ctx->band_stream[i]));
+        CK(cudaStreamWaitEvent(stream, ctx->band_join[i], 0));
+    }
     CK(cudaEventRecord(ctx->ev[2], stream));
     CK(launch_reduce(p.rl, stream));
     ctx->d2h += npx * static_cast<long long>(sizeof(bh_xyz));
@@ -667,8 +676,10 @@ void bh_gpu_destroy(bh_ctx* ctx) {
     cudaFree(ctx->d_queue);
     if (ctx->h_one) cudaFreeHost(ctx->h_one);
     if (ctx->h_readback) cudaFreeHost(ctx->h_readback);
-    if (ctx->band_stream) cudaStreamDestroy(ctx->band_stream);
-    if (ctx->band_join) cudaEventDestroy(ctx->band_join);
+    for (cudaStream_t st : ctx->band_stream)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : ctx->band_join)
+        if (ev) cudaEventDestroy(ev);
     if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
     if (ctx->stage) cudaFreeHost(ctx->stage);
     if (ctx->stage_free) cudaEventDestroy(ctx->stage_free);

@@ -708,7 +708,10 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     }
     if (P::kMixed) err2 = (double)err2f * (double)L.err_w;
     else if (L.err_w != 1.f) err2 *= (double)L.err_w;
-    double err = sqrt(err2 / 8.0);
+    // binary64: err = sqrt(err2 / 8); mixed: err holds its square (the
+    // accept test err^2 <= 1 and the controller's powers of err^2 need no
+    // square root; the root is taken in binary32 for an accepted step).
+    double err = P::kMixed ? err2 * 0.125 : sqrt(err2 / 8.0);
     if (L.bad_sc || !isfinite(err)) err = 1e10;
     if (P::kMixed && L.Lz != R(0) && (ax7.sn < R(0)) != (L.sn0 < R(0))) {
         // A ray with L_z != 0 never reaches the axis (Theta(th) < 0 near it:
@@ -720,7 +723,8 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         err = 1e10;
     }
     ++L.attempts;
-    double fac = 0.9 * P::powd(dmaxr(err, 1e-16), -kAlpha) * (double)L.errp_pow;
+    double fac = P::kMixed ? 0.9 * P::powd(dmaxr(err, 1e-32), -0.5 * kAlpha) * (double)L.errp_pow
+                           : 0.9 * P::powd(dmaxr(err, 1e-16), -kAlpha) * (double)L.errp_pow;
     fac = dclamp(fac, 0.2, 5.0);
 
     if (!(err <= 1.0)) {
@@ -868,7 +872,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         L.y[i] = yn[i];
         L.k1[i] = k7[i];
     }
-    L.err_prev = (R)dmaxr(err, 1e-4);
+    L.err_prev = P::kMixed ? (R)fmaxf(sqrtf((float)err), 1e-4f) : (R)dmaxr(err, 1e-4);
     L.errp_pow = (R)P::powd((double)L.err_prev, kBeta);
     L.h = hd * fac;
     L.c0 = ax7.cs;
