@@ -349,6 +349,27 @@ def test_step_budget_returns_budget_error(renderer):
     renderer.render(cfg)
 
 
+@pytest.mark.parametrize("stop", ["budget", "abort"])
+def test_banded_render_ends_when_the_launch_stops_early(renderer, stop):
+    """A frame of 128 rows or more goes through the row-band pipeline; when a
+    step budget or an abort stops the trace before every band's rays are
+    done, the band waits still end (each counter is raised to its band's size
+    after the trace kernels) and the call returns the launch's status."""
+    cfg = kerr_a09_i60(width=160, height=192)
+    if stop == "budget":
+        renderer.set_step_budget(5000)
+    else:
+        renderer.request_abort()
+    try:
+        with pytest.raises(BHError) as e:
+            renderer.render(cfg)
+        assert e.value.code == (abi.ERR_BUDGET if stop == "budget" else abi.ERR_ABORTED)
+    finally:
+        renderer.set_step_budget(0)
+        renderer.clear_abort()
+    assert np.isfinite(renderer.render(cfg)).all()
+
+
 def test_abort_flag_stops_the_launch(renderer):
     cfg = kerr_a09_i60(width=64, height=64)
     renderer.request_abort()
