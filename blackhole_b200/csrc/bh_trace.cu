@@ -361,8 +361,9 @@ struct TraceArgs {
     long long list_cap;      // select 1 with a list: the rays [0, list_cap) beside the binary32
                              // kernel (phase 0), the rest [list_cap, ..) after it (phase 1)
     int phase;
-    unsigned int* band_done; // finished rays per row band, or null
+    unsigned int* band_done; // finished rays per row band (or per frame), or null
     long long rays_per_band;
+    int band_by_frame;
 };
 
 template <class P>
@@ -396,7 +397,7 @@ __device__ __forceinline__ void write_hit(const TraceArgs& A, const Lane<P>& L, 
     if (A.band_done) {
         // the record is visible device-wide before its band's count moves
         __threadfence();
-        atomicAdd(&A.band_done[L.gid / A.rays_per_band], 1u);
+        atomicAdd(&A.band_done[A.band_by_frame ? (long long)L.frame : L.gid / A.rays_per_band], 1u);
     }
 }
 
@@ -887,17 +888,18 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         const double sn2 = (double)ax7.sn2, cs2 = (double)ax7.cs2, Del = (double)ax7.D;
         const double pr = (double)L.y[4], pth = (double)L.y[5];
         const double a2 = F.a2;
+        const double pt2 = pt * pt, pph2 = pph * pph, pth2 = pth * pth;
+        const double Ds = Del * sn2, Dpr = Del * pr;
         const double rpa = rn * rn + a2;
-        const double Ak = rpa * rpa - a2 * Del * sn2;
-        const double T1 = -Ak * pt * pt * sn2;
-        const double T2 = -4.0 * F.a * rn * pt * pph * sn2;
-        const double T3 = Del * Del * sn2 * pr * pr;
-        const double T4 = Del * sn2 * pth * pth;
-        const double T5 = (Del - a2 * sn2) * pph * pph;
+        const double T1 = (a2 * Ds - rpa * rpa) * (pt2 * sn2);
+        const double T2 = (-4.0 * F.a * pt * pph) * (rn * sn2);
+        const double T3 = (Ds * pr) * Dpr;
+        const double T4 = Ds * pth2;
+        const double T5 = (Del - a2 * sn2) * pph2;
         const double nrm = fabs(T1 + T2 + T3 + T4 + T5);
         const double scl = fabs(T1) + fabs(T2) + fabs(T3) + fabs(T4) + fabs(T5);
         if (nrm > (double)L.max_norm * scl) L.max_norm = (float)((scl > 0.0) ? nrm / scl : nrm);
-        const double Qs = pth * pth * sn2 + cs2 * (a2 * (0.0 - pt * pt) * sn2 + pph * pph);
+        const double Qs = pth2 * sn2 + cs2 * (pph2 - a2 * pt2 * sn2);
         const double dev = fabs(Qs - L.Q0 * sn2) * (double)L.inv_Q0;
         if (dev > (double)L.max_q * sn2) L.max_q = (float)(dev / sn2);
     }
@@ -1125,15 +1127,23 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.xing = L.xing;
     A.band_done = L.band_done;
     A.rays_per_band = L.rays_per_band > 0 ? L.rays_per_band : 1;
+    A.band_by_frame = L.band_by_frame;
     trace_kernel<P, MAXREG, JET, SURF><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
 }
 
 // Raises each band counter to its band's ray count (after the trace kernels).
-__global__ void band_release_kernel(unsigned int* band_done, int nbands, long long total, long long per_band) {
+// Bands are frames when frame_ray_end is given (their ray counts from it).
+__global__ void band_release_kernel(unsigned int* band_done, int nbands, long long total, long long per_band,
+                                    const long long* frame_ray_end) {
     for (int b = threadIdx.x; b < nbands; b += blockDim.x) {
-        const long long lo = (long long)b * per_band;
-        const long long n = (total - lo < per_band) ? total - lo : per_band;
+        long long n;
+        if (frame_ray_end) {
+            n = frame_ray_end[b] - (b ? frame_ray_end[b - 1] : 0);
+        } else {
+            const long long lo = (long long)b * per_band;
+            n = (total - lo < per_band) ? total - lo : per_band;
+        }
         atomicMax(&band_done[b], (unsigned int)(n > 0 ? n : 0));
     }
 }
@@ -1264,7 +1274,8 @@ cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
     // done (rays a budget or an abort left untraced included), so a stream
     // waiting on a band never waits past the trace.
     band_release_kernel<<<1, 256, 0, stream>>>(L.band_done, L.nbands, L.total_rays,
-                                               L.rays_per_band > 0 ? L.rays_per_band : 1);
+                                               L.rays_per_band > 0 ? L.rays_per_band : 1,
+                                               L.band_by_frame ? L.frame_ray_end : nullptr);
     return cudaGetLastError();
 }
 
