@@ -497,8 +497,7 @@ def batch_leg(r, rank, world, barrier, max_over_ranks, steps=2, warmup=1):
             "frames": len(frames), "rays_per_step": rays, "steps": steps, "warmup": warmup,
             "value": round(rays * steps / (dev_ms * 1e-3), 1) if dev_ms > 0 else None, "unit": "rays/s",
             "ms_per_step": round(dev_ms / steps, 3),
-            "timing": "device time from the captured graph's start (staging copies, trace) to the stats "
-                      "kernel's end, the per-frame shading and copies out overlapping the trace, max over ranks",
+            "timing": "device time of the captured graph (staging copies, trace, shade, stats), max over ranks",
             "e2e": {"value": round(rays * steps / wall, 1), "unit": "rays/s",
                     "api": "bh_gpu_render_batch into pinned host arrays reused across calls, wall clock"},
             "steps_per_ray": round(sum(s.steps for s in st) / max(1, sum(s.rays for s in st)), 2)}

@@ -398,8 +398,7 @@ int plan_launch(bh_ctx* ctx, std::vector<FrameParams>& frames, bh_xyz* d_pixels,
 // no host-synchronous call, so a CUDA graph can capture it.  Under capture the
 // caller records `stage_free` after the graph launch instead (an event
 // recorded during capture is not recorded again when the graph replays).
-int record_launch(bh_ctx* ctx, const Plan& p, cudaStream_t stream, bool timed, bool captured = false,
-                  bool shade = true) {
+int record_launch(bh_ctx* ctx, const Plan& p, cudaStream_t stream, bool timed, bool captured = false) {
     const int n = p.n;
     const unsigned char* s = ctx->stage;
     const size_t fbytes = static_cast<size_t>(p.nf) * sizeof(FrameParams);
@@ -413,7 +412,6 @@ int record_launch(bh_ctx* ctx, const Plan& p, cudaStream_t stream, bool timed, b
     if (timed) CK(cudaEventRecord(ctx->ev[0], stream));
     if (p.rays > 0) CK(launch_trace(p.tl, stream));
     if (timed) CK(cudaEventRecord(ctx->ev[1], stream));
-    if (!shade) return BH_OK;          // the caller shades and reduces (frame pipeline)
     CK(launch_shade(p.sl, stream));
     if (timed) CK(cudaEventRecord(ctx->ev[2], stream));
     CK(launch_reduce(p.rl, stream));
@@ -809,20 +807,6 @@ int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz
     if ((rc = plan_launch(ctx, frames, static_cast<bh_xyz*>(ctx->pixels.p), nullptr, false, p)) != BH_OK)
         return rc;
     ctx->h2d += static_cast<long long>(p.stage_bytes);
-    // With the driver's stream wait the frames are shaded and copied out one
-    // by one as the trace finishes them (the same pipeline as bh_gpu_render's
-    // row bands, a band being a frame): the graph then holds the staging
-    // copies and the trace, and the shading, copies and stats follow it.
-    const bool pipeline = ctx->wait_value32 != nullptr && n >= 2;
-    unsigned int* done = nullptr;
-    if (pipeline) {
-        if ((rc = ensure(ctx, ctx->band_done, static_cast<size_t>(n) * sizeof(unsigned int))) != BH_OK) return rc;
-        done = static_cast<unsigned int*>(ctx->band_done.p);
-        p.tl.band_done = done;
-        p.tl.band_by_frame = 1;
-        p.tl.nbands = n;
-        p.tl.rays_per_band = 1;
-    }
     std::vector<unsigned char> key(sizeof p.tl + sizeof p.sl + sizeof p.rl + sizeof(void*) + sizeof(size_t));
     {
         unsigned char* k = key.data();
@@ -839,7 +823,7 @@ int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz
         }
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        const int rrc = record_launch(ctx, p, ctx->stream, false, true, !pipeline);
+        const int rrc = record_launch(ctx, p, ctx->stream, false, true);
         const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
         if (rrc != BH_OK) {
             if (graph) cudaGraphDestroy(graph);
@@ -851,53 +835,18 @@ int bh_gpu_render_batch(bh_ctx* ctx, const bh_render_config* cfgs, int n, bh_xyz
         CK(ie);
         ctx->batch_key = key;
     }
-    if (pipeline) {
-        // The counters are cleared before the frame streams start waiting;
-        // the device time spans the trace, the shading, the frames' copies
-        // (which overlap the trace) and the stats.
-        CK(cudaMemsetAsync(done, 0, static_cast<size_t>(n) * sizeof(unsigned int), ctx->stream));
-        CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-        const int ns = std::min(n, kBandStreams);
-        for (int i = 0; i < ns; ++i) CK(cudaStreamWaitEvent(ctx->band_stream[i], ctx->ev[0], 0));
-        CK(cudaGraphLaunch(ctx->batch_exec, ctx->stream));
-        CK(cudaEventRecord(ctx->stage_free, ctx->stream));
-        size_t off = 0;
-        for (int i = 0; i < n; ++i) {
-            cudaStream_t bs = ctx->band_stream[i % ns];
-            const size_t m = static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
-            if (ctx->wait_value32(bs, reinterpret_cast<CUdeviceptr>(done + i), static_cast<cuuint32_t>(frames[i].n_rays),
-                                  CU_STREAM_WAIT_VALUE_GEQ) != CUDA_SUCCESS)
-                return fail(ctx, BH_ERR_CUDA, "stream wait on a frame of the batch failed");
-            ShadeLaunch sl = p.sl;
-            sl.pixel_lo = static_cast<long long>(off);
-            sl.total_pixels = static_cast<long long>(off + m);
-            CK(launch_shade(sl, bs));
-            CK(cudaMemcpyAsync(outs[i], static_cast<bh_xyz*>(ctx->pixels.p) + off, m * sizeof(bh_xyz),
-                               cudaMemcpyDeviceToHost, bs));
-            off += m;
-            ctx->d2h += static_cast<long long>(m * sizeof(bh_xyz));
-        }
-        for (int i = 0; i < ns; ++i) {
-            CK(cudaEventRecord(ctx->band_join[i], ctx->band_stream[i]));
-            CK(cudaStreamWaitEvent(ctx->stream, ctx->band_join[i], 0));
-        }
-        CK(launch_reduce(p.rl, ctx->stream));
-        CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-        CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    } else {
-        CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-        CK(cudaGraphLaunch(ctx->batch_exec, ctx->stream));
-        CK(cudaEventRecord(ctx->stage_free, ctx->stream));
-        CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-        CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-        size_t off = 0;
-        for (int i = 0; i < n; ++i) {
-            const size_t m = static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
-            CK(cudaMemcpyAsync(outs[i], static_cast<bh_xyz*>(ctx->pixels.p) + off, m * sizeof(bh_xyz),
-                               cudaMemcpyDeviceToHost, ctx->stream));
-            off += m;
-            ctx->d2h += static_cast<long long>(m * sizeof(bh_xyz));
-        }
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    CK(cudaGraphLaunch(ctx->batch_exec, ctx->stream));
+    CK(cudaEventRecord(ctx->stage_free, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        const size_t m = static_cast<size_t>(cfgs[i].width) * cfgs[i].height;
+        CK(cudaMemcpyAsync(outs[i], static_cast<bh_xyz*>(ctx->pixels.p) + off, m * sizeof(bh_xyz),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+        off += m;
+        ctx->d2h += static_cast<long long>(m * sizeof(bh_xyz));
     }
     CK(cudaStreamSynchronize(ctx->stream));
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -58,7 +58,6 @@ struct TraceLaunch {
     unsigned int* band_done;
     long long rays_per_band;
     int nbands;
-    int band_by_frame;               // 1: a band is a frame of the launch (counters per frame)
 };
 
 // Bytes of one deferred-ray record.

@@ -361,9 +361,8 @@ struct TraceArgs {
     long long list_cap;      // select 1 with a list: the rays [0, list_cap) beside the binary32
                              // kernel (phase 0), the rest [list_cap, ..) after it (phase 1)
     int phase;
-    unsigned int* band_done; // finished rays per row band (or per frame), or null
+    unsigned int* band_done; // finished rays per row band, or null
     long long rays_per_band;
-    int band_by_frame;
 };
 
 template <class P>
@@ -397,7 +396,7 @@ __device__ __forceinline__ void write_hit(const TraceArgs& A, const Lane<P>& L, 
     if (A.band_done) {
         // the record is visible device-wide before its band's count moves
         __threadfence();
-        atomicAdd(&A.band_done[A.band_by_frame ? (long long)L.frame : L.gid / A.rays_per_band], 1u);
+        atomicAdd(&A.band_done[L.gid / A.rays_per_band], 1u);
     }
 }
 
@@ -879,12 +878,33 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     L.c0 = ax7.cs;
     L.sn0 = ax7.sn;
 
-    {
-        // Invariant diagnostics at the new state (render.cpp:139-145), in
-        // binary64, after the events so the stage values are no longer live.
-        // The five terms of g^{ab} p_a p_b (kerr.h:301-321) are all scaled by
-        // Sigma Delta sin^2 > 0 and Carter's Q by sin^2, which leaves both
-        // ratios unchanged; a division only when a maximum grows.
+    // Invariant diagnostics at the new state (render.cpp:139-145), after
+    // the events so the stage values are no longer live.  The five terms of
+    // g^{ab} p_a p_b (kerr.h:301-321) are all scaled by Sigma Delta sin^2 > 0
+    // and Carter's Q by sin^2, which leaves both ratios unchanged; a division
+    // only when a maximum grows.  Binary64 frames evaluate them in binary64;
+    // mixed ones in binary32, from the binary32 state they measure: each term
+    // to a few ulp, so the reported ratios carry up to about 1e-6 of their
+    // own rounding.
+    if constexpr (P::kMixed) {
+        const float sn2 = ax7.sn2, cs2 = ax7.cs2, Del = ax7.D;
+        const float rf = yn[1], pr = L.y[4], pth = L.y[5];
+        const float a2 = L.a2R;
+        const float pt2 = L.E * L.E, pph2 = L.Lz2, pth2 = pth * pth;
+        const float Ds = Del * sn2, Dpr = Del * pr;
+        const float rpa = fmaf(rf, rf, a2);
+        const float T1 = fmaf(a2, Ds, -(rpa * rpa)) * (pt2 * sn2);
+        const float T2 = (4.f * L.aE * L.Lz) * (rf * sn2);
+        const float T3 = (Ds * pr) * Dpr;
+        const float T4 = Ds * pth2;
+        const float T5 = fmaf(-a2, sn2, Del) * pph2;
+        const float nrm = fabsf(T1 + T2 + T3 + T4 + T5);
+        const float scl = fabsf(T1) + fabsf(T2) + fabsf(T3) + fabsf(T4) + fabsf(T5);
+        if (nrm > L.max_norm * scl) L.max_norm = (scl > 0.f) ? nrm / scl : nrm;
+        const float Qs = fmaf(pth2, sn2, cs2 * fmaf(-L.a2E2, sn2, pph2));
+        const float dev = fabsf(fmaf(-(float)L.Q0, sn2, Qs)) * L.inv_Q0;
+        if (dev > L.max_q * sn2) L.max_q = dev / sn2;
+    } else {
         const double sn2 = (double)ax7.sn2, cs2 = (double)ax7.cs2, Del = (double)ax7.D;
         const double pr = (double)L.y[4], pth = (double)L.y[5];
         const double a2 = F.a2;
@@ -1127,23 +1147,15 @@ cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cuda
     A.xing = L.xing;
     A.band_done = L.band_done;
     A.rays_per_band = L.rays_per_band > 0 ? L.rays_per_band : 1;
-    A.band_by_frame = L.band_by_frame;
     trace_kernel<P, MAXREG, JET, SURF><<<grid, block, 0, s>>>(A);
     return cudaGetLastError();
 }
 
 // Raises each band counter to its band's ray count (after the trace kernels).
-// Bands are frames when frame_ray_end is given (their ray counts from it).
-__global__ void band_release_kernel(unsigned int* band_done, int nbands, long long total, long long per_band,
-                                    const long long* frame_ray_end) {
+__global__ void band_release_kernel(unsigned int* band_done, int nbands, long long total, long long per_band) {
     for (int b = threadIdx.x; b < nbands; b += blockDim.x) {
-        long long n;
-        if (frame_ray_end) {
-            n = frame_ray_end[b] - (b ? frame_ray_end[b - 1] : 0);
-        } else {
-            const long long lo = (long long)b * per_band;
-            n = (total - lo < per_band) ? total - lo : per_band;
-        }
+        const long long lo = (long long)b * per_band;
+        const long long n = (total - lo < per_band) ? total - lo : per_band;
         atomicMax(&band_done[b], (unsigned int)(n > 0 ? n : 0));
     }
 }
@@ -1274,8 +1286,7 @@ cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
     // done (rays a budget or an abort left untraced included), so a stream
     // waiting on a band never waits past the trace.
     band_release_kernel<<<1, 256, 0, stream>>>(L.band_done, L.nbands, L.total_rays,
-                                               L.rays_per_band > 0 ? L.rays_per_band : 1,
-                                               L.band_by_frame ? L.frame_ray_end : nullptr);
+                                               L.rays_per_band > 0 ? L.rays_per_band : 1);
     return cudaGetLastError();
 }
 
