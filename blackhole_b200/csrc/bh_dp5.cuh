@@ -28,6 +28,7 @@ constexpr double D1 = -12715105075.0 / 11282082432.0, D3 = 87487479700.0 / 32700
                  D6 = -1453857185.0 / 822651844.0, D7 = 69997945.0 / 29380423.0;
 // PI controller (Gustafsson): alpha = 0.7/5, beta = 0.4/5, safety 0.9, [0.2, 5].
 constexpr double kAlpha = 0.7 / 5.0, kBeta = 0.4 / 5.0;
+constexpr double kLnErrFloor = -9.210340371976184;   // ln 1e-4, the floor of err_prev
 
 // Dense-output polynomial of one component (geodesic.h:109-121, 176-185).
 struct DenseC { double r1, r2, r3, r4, r5; };
