@@ -6,7 +6,7 @@
 //
 //   1. forward: the ray is integrated with the render path's DP5(4) scheme,
 //      PI controller, step limiter and events (render.cpp:69-260,
-//      geodesic.h:123-204); the state (y, h, err_prev) after every
+//      geodesic.h:123-204); the state (y, h, controller memory) after every
 //      `interval` accepted steps is stored in the ray's checkpoint slots.
 //      When the slots are full every second checkpoint is dropped and the
 //      interval doubles, so memory stays bounded for any step count;
@@ -276,7 +276,8 @@ __host__ __device__ BHA_NOINLINE void rhs6_vjp(const RayC& c, double r, double s
 struct Integ {
     double y[6];        // t, r, th, phi, p_r, p_th
     double k1[6];       // FSAL stage at y
-    double h, err_prev;
+    double h;
+    double errp_mem;    // beta ln err_prev, err_prev the last accepted error norm (>= 1e-4)
     double c0;          // cos(th) at y
     int have_k1;
     int tries;
@@ -337,9 +338,13 @@ __host__ __device__ BHA_NOINLINE bool advance(const FrameParams& F, const RayC& 
             const double q = e / scl;
             err2 += q * q;
         }
-        double err = sqrt(err2 / 8.0);
+        // err: the square of the RMS norm; the PI factor 0.9 err^-alpha
+        // err_prev^beta (geodesic.h:171-173) as one exp of logarithms, the
+        // forward pass and every replay alike
+        double err = err2 * 0.125;
         if (!is_finite(err)) err = 1e10;
-        double fac = 0.9 * pow(dmaxr(err, 1e-16), -kAlpha) * pow(dmaxr(s.err_prev, 1e-4), kBeta);
+        const double lq = log(dmaxr(err, 1e-32));
+        double fac = 0.9 * exp(fma(-0.5 * kAlpha, lq, s.errp_mem));
         fac = dclamp(fac, 0.2, 5.0);
         if (!(err <= 1.0)) {
             s.h *= dminr(fac, 1.0);
@@ -366,7 +371,7 @@ __host__ __device__ BHA_NOINLINE bool advance(const FrameParams& F, const RayC& 
             s.k1[i] = k[6][i];
         }
         s.c0 = c7;
-        s.err_prev = dmaxr(err, 1e-4);
+        s.errp_mem = kBeta * dmaxr(0.5 * lq, kLnErrFloor);
         s.h = h * fac;
         return true;
     }
@@ -788,7 +793,7 @@ __host__ __device__ inline void ray_start(const FrameParams& F, const AdjointFra
 // in pieces of at most this many steps.
 constexpr int kReplay = 16;
 
-// Checkpoint store of one ray: `slots` states of 8 doubles (y, h, err_prev)
+// Checkpoint store of one ray: `slots` states of 8 doubles (y, h, beta ln err_prev)
 // after every `interval` accepted steps; full slots drop every second state
 // and double the interval.
 struct Checkpoints {
@@ -800,7 +805,7 @@ struct Checkpoints {
         double* p = ck + 8 * n;
         for (int i = 0; i < 6; ++i) p[i] = st.y[i];
         p[6] = st.h;
-        p[7] = st.err_prev;
+        p[7] = st.errp_mem;
         ++n;
     }
     __host__ __device__ void after_step(const Integ& st) {
@@ -889,7 +894,7 @@ __host__ __device__ inline long long reverse_sweep(const FrameParams& F, const R
             const double* p = cp.ck + 8 * seg;
             for (int i = 0; i < 6; ++i) r.y[i] = p[i];
             r.h = p[6];
-            r.err_prev = p[7];
+            r.errp_mem = p[7];
             r.have_k1 = 0;
             r.tries = 0;
             r.steps = 0;
@@ -926,7 +931,7 @@ __host__ __device__ inline RayC ray_consts(const FrameParams& F, double E, doubl
 __host__ __device__ inline void integ_start(const FrameParams& F, const double y0[6], Integ& s) {
     for (int i = 0; i < 6; ++i) s.y[i] = y0[i];
     s.h = F.h0;
-    s.err_prev = 1e-4;
+    s.errp_mem = kBeta * kLnErrFloor;
     s.have_k1 = 0;
     s.tries = 0;
     s.steps = 0;
