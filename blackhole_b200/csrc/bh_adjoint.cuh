@@ -129,7 +129,7 @@ __host__ __device__ BHA_NOINLINE void rhs6(const RayC& c, double r, double sn, d
     const double sn2 = sn * sn, cs2 = cs * cs, r2 = r * r;
     const double S = r2 + c.a2 * cs2;
     const double D = c.factored ? (r - c.rp) * (r - c.rm) : (r2 - 2.0 * r + c.a2);
-    const double inv = 1.0 / (S * D * sn2);
+    const double inv = rcp_nr(S * D * sn2);
     const double iS = inv * D * sn2, iD = inv * S * sn2, isn2 = inv * S * D;
     const double r2a2 = r2 + c.a2;
     const double K = r2a2 * c.E - c.a * c.Lz;
@@ -169,7 +169,7 @@ __host__ __device__ BHA_NOINLINE void rhs6_vjp(const RayC& c, double r, double s
     const double sn2 = sn * sn, cs2 = cs * cs, r2 = r * r;
     const double S = r2 + a2 * cs2;
     const double D = c.factored ? (r - c.rp) * (r - c.rm) : (r2 - 2.0 * r + a2);
-    const double inv = 1.0 / (S * D * sn2);
+    const double inv = rcp_nr(S * D * sn2);
     const double iS = inv * D * sn2, iD = inv * S * sn2, isn2 = inv * S * D;
     const double r2a2 = r2 + a2;
     const double K = r2a2 * E - a * Lz;
@@ -335,7 +335,7 @@ __host__ __device__ BHA_NOINLINE bool advance(const FrameParams& F, const RayC& 
             const double e = h * (E1 * k[0][i] + E3 * k[2][i] + E4 * k[3][i] + E5 * k[4][i] + E6 * k[5][i] +
                                   E7 * k[6][i]);
             const double scl = F.atol + F.rtol * dmaxr(fabs(s.y[i]), fabs(yn[i]));
-            const double q = e / scl;
+            const double q = e * rcp_nr(scl);
             err2 += q * q;
         }
         // err: the square of the RMS norm; the PI factor 0.9 err^-alpha

@@ -18,6 +18,24 @@ __host__ __device__ __forceinline__ double dclamp(double v, double lo, double hi
     return (v < lo) ? lo : (hi < v) ? hi : v;
 }
 
+// 1 / x in binary64 from the hardware's approximate reciprocal and two Newton
+// steps e = 1 - x r, r += r e (the error squares each step, ending within an
+// ulp): a handful of fused multiply-adds instead of the division sequence.
+// x = 0 gives NaN where the division gives inf; both make the step
+// non-finite, which the controller rejects.  Host code: the division.
+__host__ __device__ __forceinline__ double rcp_nr(double x) {
+#if defined(__CUDA_ARCH__)
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+#else
+    return 1.0 / x;
+#endif
+}
+
 // splitmix64 output of state z (scene.h:30-36) and its 53-bit uniform (scene.h:37).
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;

@@ -41,7 +41,7 @@ struct Fp64 {
     using R = double;
     static constexpr bool kMixed = false;
     __device__ static __forceinline__ void sc(double x, double* s, double* c) { sincos(x, s, c); }
-    __device__ static __forceinline__ double rcp(double x) { return 1.0 / x; }
+    __device__ static __forceinline__ double rcp(double x) { return rcp_nr(x); }
     __device__ static __forceinline__ double powd(double x, double y) { return pow(x, y); }
 };
 
@@ -713,7 +713,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             err2f += q * q;
         } else {
             const double sc = F.atol + F.rtol * dmaxr(fabs((double)L.y[i]), fabs((double)yn[i]));
-            const double q = (double)e / sc;
+            const double q = (double)e * rcp_nr(sc);
             err2 += q * q;
         }
     }
