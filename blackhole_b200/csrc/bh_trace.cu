@@ -257,9 +257,11 @@ __device__ __forceinline__ void rhs_sc(const Lane<P>& L, typename P::R r, typena
     }
 }
 
-// The full sin/cos of a stage whose angle moved more than kMaxShift: rare, so
-// out of line (inlined in five stages it kept the step loop from staying in
-// the instruction cache: -2% per frame in both precisions).
+// The full sin/cos of an angle that angle addition from the step's base angle
+// does not reach: a stage whose angle moved more than kMaxShift (and, in
+// binary64, a ray's first angle or a step's end that moved that far).  Rare,
+// so out of line: inlined in five stages it kept the step loop from staying
+// in the instruction cache (-2% per frame in both precisions).
 template <class P>
 __device__ __noinline__ void stage_sincos_far(typename P::R th, typename P::R* sn, typename P::R* cs) {
     P::sc(th, sn, cs);
@@ -601,7 +603,14 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     }
     if (!L.have_k1) {
         Aux<P> ax;
-        rhs<P>(L, L.y[1], L.y[2], L.y[4], L.y[5], L.k1, &ax);
+        if constexpr (P::kMixed) {
+            rhs<P>(L, L.y[1], L.y[2], L.y[4], L.y[5], L.k1, &ax);
+        } else {
+            // binary64: no full sin/cos inline in the step loop (below)
+            double sn, cs;
+            stage_sincos_far<P>(L.y[2], &sn, &cs);
+            rhs_sc<P>(L, L.y[1], sn, cs, L.y[4], L.y[5], L.k1, &ax);
+        }
         L.c0 = ax.cs;
         L.sn0 = ax.sn;
         L.have_k1 = 1;
@@ -678,9 +687,20 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
                                   R(B6) * k6[i]);
     }
     // The last stage is the next step's first (FSAL) and its angle the next
-    // base angle: full sincos, so angle-addition errors never chain.
+    // base angle.  binary32: full sincos, so angle-addition errors never
+    // chain.  binary64: by angle addition from the step's base angle like the
+    // stages (a chain of ulp-sized roundings, ~1e-15 after a thousand steps),
+    // which keeps the full sin/cos out of the step loop (-1.7% per frame).
     Aux<P> ax7;
-    rhs<P>(L, yn[1], yn[2], yn[4], yn[5], k7, &ax7);
+    if constexpr (P::kMixed) {
+        rhs<P>(L, yn[1], yn[2], yn[4], yn[5], k7, &ax7);
+    } else {
+        const double dth = yn[2] - L.y[2];
+        double sn, cs;
+        if (fabs(dth) <= kMaxShift) shift_sincos(L.sn0, L.c0, dth, &sn, &cs);
+        else stage_sincos_far<P>(yn[2], &sn, &cs);
+        rhs_sc<P>(L, yn[1], sn, cs, yn[4], yn[5], k7, &ax7);
+    }
 
     // RMS error over the eight components (geodesic.h:157-166): the p_t and
     // p_phi terms are exactly zero.  binary64: squares summed in binary64;
