@@ -36,6 +36,33 @@ __host__ __device__ __forceinline__ double rcp_nr(double x) {
 #endif
 }
 
+// sin and cos of th0 + d from those of th0, |d| <= kMaxShift: angle addition
+// with the Taylor series of sin d and cos d in Horner form (coefficients
+// +-1/n!): to d^7 / d^6 in binary32, to d^13 / d^14 in binary64 (truncation
+// below the format's rounding for |d| <= 1/4).
+constexpr double kMaxShift = 0.25;
+__host__ __device__ __forceinline__ void shift_sincos(float s0, float c0, float d, float* s, float* c) {
+    const float d2 = d * d;
+    const float ps = fmaf(d2, fmaf(d2, -1.f / 5040.f, 1.f / 120.f), -1.f / 6.f);
+    const float pc = fmaf(d2, fmaf(d2, -1.f / 720.f, 1.f / 24.f), -0.5f);
+    const float sd = fmaf(d * d2, ps, d);
+    const float cd = fmaf(d2, pc, 1.f);
+    *s = fmaf(s0, cd, c0 * sd);
+    *c = fmaf(c0, cd, -(s0 * sd));
+}
+__host__ __device__ __forceinline__ void shift_sincos(double s0, double c0, double d, double* s, double* c) {
+    const double d2 = d * d;
+    const double ps = fma(d2, fma(d2, fma(d2, fma(d2, fma(d2, 1.0 / 6227020800.0, -1.0 / 39916800.0),
+                                              1.0 / 362880.0), -1.0 / 5040.0), 1.0 / 120.0), -1.0 / 6.0);
+    const double pc = fma(d2, fma(d2, fma(d2, fma(d2, fma(d2, fma(d2, -1.0 / 87178291200.0, 1.0 / 479001600.0),
+                                                      -1.0 / 3628800.0), 1.0 / 40320.0), -1.0 / 720.0),
+                              1.0 / 24.0), -0.5);
+    const double sd = fma(d * d2, ps, d);
+    const double cd = fma(d2, pc, 1.0);
+    *s = fma(s0, cd, c0 * sd);
+    *c = fma(c0, cd, -(s0 * sd));
+}
+
 // splitmix64 output of state z (scene.h:30-36) and its 53-bit uniform (scene.h:37).
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;

@@ -152,36 +152,6 @@ struct Aux {
     typename P::R sn, cs, sn2, cs2, D;
 };
 
-// sin and cos of th0 + d from those of th0, |d| <= kMaxShift: angle addition
-// with Taylor series of sin d and cos d (to d^7 / d^6 in binary32, d^13 /
-// d^14 in binary64: truncation below the format's rounding for |d| <= 1/4).
-constexpr double kMaxShift = 0.25;
-
-__device__ __forceinline__ void shift_sincos(float s0, float c0, float d, float* s, float* c) {
-    // sin d = d + d^3 (-1/6 + d^2 (1/120 - d^2 / 5040)),
-    // cos d = 1 + d^2 (-1/2 + d^2 (1/24 - d^2 / 720)), in Horner form
-    const float d2 = d * d;
-    const float ps = fmaf(d2, fmaf(d2, -1.f / 5040.f, 1.f / 120.f), -1.f / 6.f);
-    const float pc = fmaf(d2, fmaf(d2, -1.f / 720.f, 1.f / 24.f), -0.5f);
-    const float sd = fmaf(d * d2, ps, d);
-    const float cd = fmaf(d2, pc, 1.f);
-    *s = fmaf(s0, cd, c0 * sd);
-    *c = fmaf(c0, cd, -(s0 * sd));
-}
-__device__ __forceinline__ void shift_sincos(double s0, double c0, double d, double* s, double* c) {
-    // reciprocals as constants: a division by 6.0 is a real division
-    constexpr double i6 = 1.0 / 6.0, i20 = 1.0 / 20.0, i42 = 1.0 / 42.0, i72 = 1.0 / 72.0;
-    constexpr double i110 = 1.0 / 110.0, i156 = 1.0 / 156.0;
-    constexpr double i12 = 1.0 / 12.0, i30 = 1.0 / 30.0, i56 = 1.0 / 56.0, i90 = 1.0 / 90.0;
-    constexpr double i132 = 1.0 / 132.0, i182 = 1.0 / 182.0;
-    const double d2 = d * d;
-    const double sd = d * (1.0 - d2 * i6 * (1.0 - d2 * i20 * (1.0 - d2 * i42 * (1.0 - d2 * i72 *
-                      (1.0 - d2 * i110 * (1.0 - d2 * i156))))));
-    const double cd = 1.0 - d2 * 0.5 * (1.0 - d2 * i12 * (1.0 - d2 * i30 * (1.0 - d2 * i56 *
-                      (1.0 - d2 * i90 * (1.0 - d2 * i132 * (1.0 - d2 * i182))))));
-    *s = s0 * cd + c0 * sd;
-    *c = c0 * cd - s0 * sd;
-}
 
 // ---- packed binary32 pairs ----------------------------------------------------
 // sm_100's f32x2 arithmetic: one instruction does the same binary32 operation,
