@@ -27,6 +27,10 @@ struct FrameParams {
     double r_promote;                // innermost photon orbit: an ingoing ray below it is falling in
     double land_limit, land_target;  // mixed: a step from inside r_escape that would end beyond land_limit
                                      // is shortened to end near land_target (see land_escape)
+    // binary32 copies of the constants the mixed kernel's step control reads
+    // every attempt (no conversion in the step loop)
+    float f_hmax_a, f_hmax_b, f_r_h, f_atol, f_rtol;
+    float f_land_limit, f_r_stop, f_r_escape, f_r_promote, f_pad;
     int32_t early_capture;           // mixed: end such a ray as captured there
     int32_t mirror_ok;               // mixed: integrate th > pi/2 as its mirror pi - th
     int32_t fp64_near_critical;      // mixed: near-critical rays traced in binary64

@@ -291,6 +291,22 @@ int star_catalogue(int count, uint64_t seed, int sky_mode, double* out6) {
     return BH_OK;
 }
 
+namespace {
+// The binary32 copies of F's step-control constants (FrameParams::f_*).
+void set_binary32_copies(FrameParams& F) {
+    F.f_hmax_a = static_cast<float>(F.hmax_a);
+    F.f_hmax_b = static_cast<float>(F.hmax_b);
+    F.f_r_h = static_cast<float>(F.r_h);
+    F.f_atol = static_cast<float>(F.atol);
+    F.f_rtol = static_cast<float>(F.rtol);
+    F.f_land_limit = static_cast<float>(F.land_limit);
+    F.f_r_stop = static_cast<float>(F.r_stop);
+    F.f_r_escape = static_cast<float>(F.r_escape);
+    F.f_r_promote = static_cast<float>(F.r_promote);
+    F.f_pad = 0.f;
+}
+}  // namespace
+
 int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     std::memset(&F, 0, sizeof F);
     if (c.width <= 0 || c.height <= 0) { err = "width and height must be positive"; return BH_ERR_INVALID_ARG; }
@@ -394,6 +410,7 @@ int make_frame(const bh_render_config& c, FrameParams& F, std::string& err) {
     // turning point left and falls into the hole.
     F.r_promote = (F.a2 < 1.0) ? 2.0 * (1.0 + std::cos((2.0 / 3.0) * std::acos(-std::fabs(a)))) : 0.0;
     F.max_steps = c.max_steps;
+    set_binary32_copies(F);
 
     // Camera (scene.h:356-384, render.cpp:409-414).
     F.cam_r = c.cam.r;
@@ -549,6 +566,7 @@ FrameParams binary64_treatment(const FrameParams& F) {
     G.land_escape = 0;
     G.early_capture = 0;
     G.mirror_ok = 0;
+    set_binary32_copies(G);
     return G;
 }
 

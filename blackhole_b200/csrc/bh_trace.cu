@@ -130,7 +130,7 @@ struct Lane {
     R rp_hi, rp_lo, rm_hi, rm_lo;   // r_+ and r_- as exact two-term sums
     R c0;                    // cos(th) at y (disc-plane test, stage angles)
     R sn0;                   // sin(th) at y as the metric clamps it (stage angles)
-    double h;
+    R h;
     R err_prev;              // PI-controller memory: the last accepted error norm
     R errp_mem;              // its factor: pow(err_prev, beta) (binary32 lanes),
                              // beta ln err_prev (binary64 lanes)
@@ -568,8 +568,13 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     using R = typename P::R;
     const FrameParams& F = A.frames[L.frame];
     if (L.tries == 0) {
-        const double hmax = F.hmax_a * dmaxr(1.0, (double)L.y[1] - F.r_h) + F.hmax_b;
-        if (L.h > hmax) L.h = hmax;
+        if constexpr (P::kMixed) {
+            const float hmax = fmaf(F.f_hmax_a, fmaxf(1.f, L.y[1] - F.f_r_h), F.f_hmax_b);
+            if (L.h > hmax) L.h = hmax;
+        } else {
+            const double hmax = F.hmax_a * dmaxr(1.0, L.y[1] - F.r_h) + F.hmax_b;
+            if (L.h > hmax) L.h = hmax;
+        }
     }
     if (!L.have_k1) {
         Aux<P> ax;
@@ -586,12 +591,12 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         L.have_k1 = 1;
     }
     if (L.tries == 0 && F.land_escape && L.k1[1] > typename P::R(0) &&
-        (float)L.y[1] + (float)L.h * (float)L.k1[1] > (float)F.land_limit && (double)L.y[1] < F.r_escape) {
+        (float)L.y[1] + (float)L.h * (float)L.k1[1] > F.f_land_limit && (double)L.y[1] < F.r_escape) {
         // An escaping step lands within the reference's cap of r_escape: a
         // step predicted (to first order) to end beyond land_limit ends near
         // land_target instead, as it would under the reference's step cap.
         const double hl = (F.land_target - (double)L.y[1]) / (double)L.k1[1];
-        if (hl > 0.0 && hl < L.h) L.h = hl;
+        if (hl > 0.0 && hl < (double)L.h) L.h = (R)hl;
     }
     const R h = (R)L.h;
     R t[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], yn[6];
@@ -674,8 +679,10 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
 
     // RMS error over the eight components (geodesic.h:157-166): the p_t and
     // p_phi terms are exactly zero.  binary64: squares summed in binary64;
-    // mixed: scaled errors and their squares in binary32, the norm and the
-    // accept/reject test in binary64.
+    // mixed: the scaled errors, the norm, the accept/reject test and the step
+    // control in binary32 (a binary64 step control converted between the
+    // formats about twenty times per attempt: 3.38 against 3.16 ms per 1024^2
+    // frame).
     double err2 = 0.0;
     float err2f = 0.f;
     R ev[6];
@@ -697,8 +704,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             // more steps than the same scene turned about the axis)
             const float y0 = (i == 2 && L.mirror) ? kPiHi - (float)L.y[i] : (float)L.y[i];
             const float y1 = (i == 2 && L.mirror) ? kPiHi - (float)yn[i] : (float)yn[i];
-            const float sc = (i == 3) ? (float)F.atol + (float)F.rtol
-                                      : (float)F.atol + (float)F.rtol * fmaxf(fabsf(y0), fabsf(y1));
+            const float sc = (i == 3) ? F.f_atol + F.f_rtol : F.f_atol + F.f_rtol * fmaxf(fabsf(y0), fabsf(y1));
             const float q = (float)e * Mixed::rcp(sc);
             err2f += q * q;
         } else {
@@ -707,12 +713,17 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             err2 += q * q;
         }
     }
-    if (P::kMixed) err2 = (double)err2f * (double)L.err_w;
-    else if (L.err_w != 1.f) err2 *= (double)L.err_w;
     // err holds the square of the RMS norm sqrt(err2 / 8): the accept test
     // err^2 <= 1 and the controller's powers of err^2 need no square root.
-    double err = err2 * 0.125;
-    if (L.bad_sc || !isfinite(err)) err = 1e10;
+    // The step control runs in the lane's precision.
+    R err;
+    if constexpr (P::kMixed) {
+        err = err2f * L.err_w * 0.125f;
+    } else {
+        if (L.err_w != 1.f) err2 *= (double)L.err_w;
+        err = err2 * 0.125;
+    }
+    if (L.bad_sc || !isfinite(err)) err = R(1e10);
     if (P::kMixed && L.Lz != R(0) && (ax7.sn < R(0)) != (L.sn0 < R(0))) {
         // A ray with L_z != 0 never reaches the axis (Theta(th) < 0 near it:
         // it turns at th_min ~ |L_z| / sqrt(Q + a^2 E^2)).  A binary32 step
@@ -720,7 +731,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         // L_z^2 / sin^3 force changes over th_min / p_th of affine parameter
         // and atol alone bounds the error in th: rejected, so the steps
         // shrink until they resolve the turn.
-        err = 1e10;
+        err = R(1e10);
     }
     ++L.attempts;
     // The PI step factor 0.9 err^-alpha err_prev^beta (geodesic.h:171-173):
@@ -728,18 +739,19 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     // beta ln err_prev - alpha ln err, the logarithm of this attempt's norm
     // kept for the next step (binary64 pow is a long extended-precision
     // sequence, and the factor only sets the next step's size).
-    double fac, lq = 0.0;
+    R fac;
+    double lq = 0.0;
     if constexpr (P::kMixed) {
-        fac = 0.9 * P::powd(dmaxr(err, 1e-32), -0.5 * kAlpha) * (double)L.errp_mem;
+        fac = 0.9f * __powf(fmaxf(err, 1e-32f), (float)(-0.5 * kAlpha)) * L.errp_mem;
     } else {
         lq = log(dmaxr(err, 1e-32));
-        fac = 0.9 * exp(fma(-0.5 * kAlpha, lq, (double)L.errp_mem));
+        fac = 0.9 * exp(fma(-0.5 * kAlpha, lq, L.errp_mem));
     }
-    fac = dclamp(fac, 0.2, 5.0);
+    fac = (fac < R(0.2)) ? R(0.2) : (R(5) < fac) ? R(5) : fac;   // std::clamp(fac, 0.2, 5)
 
-    if (!(err <= 1.0)) {
-        L.h *= dminr(fac, 1.0);
-        if (++L.tries > 40 || fabs(L.h) < 1e-14) {
+    if (!(err <= R(1))) {
+        L.h *= (R(1) < fac) ? R(1) : fac;
+        if (++L.tries > 40 || fabs(L.h) < R(1e-14)) {
             // render.cpp:133-136: no acceptable step is a capture, reported
             // with the ray's initial state.
             double y8[8], Q0;
@@ -756,6 +768,13 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     const double rn = (double)yn[1];
     const double pt = -(double)L.E, pph = (double)L.Lz;
     const double hd = L.h;
+    // the mixed kernel's stop radii in binary32 (the binary64 one reads F's)
+    float r_stop_f = 0.f, r_escape_f = 0.f, r_promote_f = 0.f;
+    if constexpr (P::kMixed) {
+        r_stop_f = F.f_r_stop;
+        r_escape_f = F.f_r_escape;
+        r_promote_f = F.f_r_promote;
+    }
     const double ptph[2] = {pt, pph};
     int what = -1;
     double yh[8];
@@ -785,9 +804,10 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         what = BH_HIT_STAR;
         s_jet = dense_crossing(cr, F.ns_R);
         dense_state(s_jet);
-    } else if (rn <= F.r_stop) {
+    } else if (P::kMixed ? yn[1] <= r_stop_f : rn <= F.r_stop) {
         what = BH_HIT_HORIZON;             // render.cpp:172-177
-    } else if (F.disc_enabled && (double)L.c0 * (double)ax7.cs < 0.0) {
+    } else if (F.disc_enabled && (P::kMixed ? ((L.c0 < R(0)) && (ax7.cs > R(0))) || ((L.c0 > R(0)) && (ax7.cs < R(0)))
+                                            : (double)L.c0 * (double)ax7.cs < 0.0)) {
         // equatorial crossing (render.cpp:180-199): cos(th) changes sign at
         // th* = pi/2 + m pi between th(0) and th(1)
         const DenseC cth = dense_coef(hd, L.y[2], yn[2], L.k1[2], k3[2], k4[2], k5[2], k6[2], k7[2]);
@@ -874,7 +894,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             L.jet += jet_step_integral(F, cr, ct, cpr, cpt, (double)L.E, (double)L.Lz, hd, s_jet);
         }
     }
-    if (what < 0 && rn > F.r_escape) what = BH_HIT_SKY;   // render.cpp:247-251
+    if (what < 0 && (P::kMixed ? yn[1] > r_escape_f : rn > F.r_escape)) what = BH_HIT_SKY;   // render.cpp:247-251
 
     // Advance; FSAL: k7 becomes the next k1.
     #pragma unroll
@@ -883,12 +903,12 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         L.k1[i] = k7[i];
     }
     if constexpr (P::kMixed) {
-        L.err_prev = (R)fmaxf(sqrtf((float)err), 1e-4f);
-        L.errp_mem = (R)P::powd((double)L.err_prev, kBeta);
+        L.err_prev = fmaxf(sqrtf(err), 1e-4f);
+        L.errp_mem = __powf(L.err_prev, (float)kBeta);
     } else {
         L.errp_mem = kBeta * dmaxr(0.5 * lq, kLnErrFloor);   // err_prev >= 1e-4
     }
-    L.h = hd * fac;
+    L.h = P::kMixed ? L.h * fac : (R)(hd * fac);
     L.c0 = ax7.cs;
     L.sn0 = ax7.sn;
 
@@ -944,7 +964,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         what = BH_HIT_EXHAUSTED;
         state8(L, ptph, yh);
     }
-    if (what < 0 && F.early_capture && rn < F.r_promote && k7[1] < R(0)) {
+    if (what < 0 && F.early_capture && (P::kMixed ? yn[1] < r_promote_f : rn < F.r_promote) && k7[1] < R(0)) {
         // Moving inwards inside the innermost photon orbit: no radial turning
         // point is left, the ray falls into the hole, and nothing lies on
         // its way (no neutron star, no jet; the disc is outside the ISCO).
@@ -962,7 +982,8 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
         return true;
     }
     if (P::kMixed && A.deferred &&
-        ((rn < F.r_promote && k7[1] < R(0)) || (!F.mirror_ok && ax7.sn2 < R(kPoleSin2)))) {
+        (((P::kMixed ? yn[1] < r_promote_f : rn < F.r_promote) && k7[1] < R(0)) ||
+         (!F.mirror_ok && ax7.sn2 < R(kPoleSin2)))) {
         // Two places where binary32 state cannot carry the geodesic, handed
         // to the binary64 kernel for the rest of the ray:
         //  - moving inwards inside the innermost photon orbit: the ray is
