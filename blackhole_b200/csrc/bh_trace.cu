@@ -572,12 +572,19 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     return true;
 }
 
+// What a trace kernel is compiled with beyond the integration and the
+// horizon, disc and escape events: nothing; the Sun's and the neutron star's
+// surface tests and the record of equatorial crossings; the crossing record
+// alone (the discrete adjoint's render).
+enum { kSurfNone = 0, kSurfAll = 1, kSurfCrossings = 2 };
+constexpr int kFamily = 4;   // trace kernels of a precision and register cap
+
 // One step attempt.  Returns true when the lane's ray is finished here
-// (terminated, or deferred to the binary64 kernel).  SURF: compiled with the
-// Sun's and the neutron star's surface tests and the record of equatorial
-// crossings; launches that need none of them run kernels without that code
-// (taken by no lane, it still costs instruction-cache room and registers).
-template <class P, bool JET, bool SURF>
+// (terminated, or deferred to the binary64 kernel).  SURF (kSurf*): what the
+// kernel is compiled with besides the horizon, disc and escape events;
+// launches run the kernel with no more than they need (code taken by no lane
+// still costs instruction-cache room and registers).
+template <class P, bool JET, int SURF>
 __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     using R = typename P::R;
     const FrameParams& F = A.frames[L.frame];
@@ -814,7 +821,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     // Fraction of the step the jet integral covers: up to an occluding
     // event, all of it otherwise; < 0: none (render.cpp:107-122, 165-244).
     double s_jet = 1.0;
-    if (SURF && F.ns_enabled && rn <= F.ns_R) {
+    if (SURF == kSurfAll && F.ns_enabled && rn <= F.ns_R) {
         // neutron-star surface (render.cpp:158-169)
         const DenseC cr = dense_coef(hd, L.y[1], yn[1], L.k1[1], k3[1], k4[1], k5[1], k6[1], k7[1]);
         what = BH_HIT_STAR;
@@ -844,7 +851,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             dense_state(s_end);
         }
     }
-    if (SURF && what < 0 && F.sun_enabled) {
+    if (SURF == kSurfAll && what < 0 && F.sun_enabled) {
         // The Sun (render.cpp:201-241): probe the dense geodesic, then bisect.
         const double a = F.a;
         auto cart = [&](double r, double th, double ph, double q[3]) {
@@ -1035,7 +1042,7 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
     return false;
 }
 
-template <class P, int MAXREG, bool JET, bool SURF>
+template <class P, int MAXREG, bool JET, int SURF>
 __global__ void __maxnreg__(MAXREG) trace_kernel(TraceArgs A) {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -1166,7 +1173,7 @@ __global__ void eval_rhs_kernel(const FrameParams* __restrict__ Fp, const double
     o[7] = 0.0;
 }
 
-template <class P, int MAXREG, bool JET, bool SURF>
+template <class P, int MAXREG, bool JET, int SURF>
 cudaError_t launch_t(const TraceLaunch& L, int resume, int grid, int block, cudaStream_t s, int select = 0,
                      int phase = 0) {
     TraceArgs A;
@@ -1227,16 +1234,18 @@ __global__ void classify_kernel(const FrameParams* __restrict__ frames, const lo
     }
 }
 
-// The three kernels of a precision and register cap: plain, with the surface
-// tests and the crossing record, with those and the jet's emission.
+// The kernels of a precision and register cap: plain, with the surface tests
+// and the crossing record, with those and the jet's emission, with the
+// crossing record alone.
 template <class P, int MAXREG>
-void family(const void* k[3]) {
-    k[0] = (const void*)trace_kernel<P, MAXREG, false, false>;
-    k[1] = (const void*)trace_kernel<P, MAXREG, false, true>;
-    k[2] = (const void*)trace_kernel<P, MAXREG, true, true>;
+void family(const void* k[kFamily]) {
+    k[0] = (const void*)trace_kernel<P, MAXREG, false, kSurfNone>;
+    k[1] = (const void*)trace_kernel<P, MAXREG, false, kSurfAll>;
+    k[2] = (const void*)trace_kernel<P, MAXREG, true, kSurfAll>;
+    k[3] = (const void*)trace_kernel<P, MAXREG, false, kSurfCrossings>;
 }
 
-void kernels_of(int precision, int variant, const void* k[3]) {
+void kernels_of(int precision, int variant, const void* k[kFamily]) {
     if (precision == BH_PRECISION_MIXED) {
         if (variant) family<Mixed, kRegMixedWide>(k);
         else family<Mixed, kRegMixed>(k);
@@ -1246,17 +1255,18 @@ void kernels_of(int precision, int variant, const void* k[3]) {
     }
 }
 
-// The kernels of launches with a jet accumulate its emission per ray, and
-// those of launches with the Sun, a neutron star or a crossing record test
-// for the surfaces and record the crossings; the others are compiled without
-// that code.
-template <bool JET, bool SURF>
+// The kernels of launches with a jet accumulate its emission per ray, those
+// of launches with the Sun or a neutron star test for the surfaces and record
+// the crossings, those of the adjoint's render record the crossings alone
+// (without the surface tests' code: 1.3% per gradient); the others are
+// compiled without that code.
+template <bool JET, int SURF>
 cudaError_t launch_fp64(const TraceLaunch& L, int resume, int grid, int block, int variant, cudaStream_t s) {
     return variant ? launch_t<Fp64, kRegFp64Wide, JET, SURF>(L, resume, grid, block, s)
                    : launch_t<Fp64, kRegFp64, JET, SURF>(L, resume, grid, block, s);
 }
 
-template <bool JET, bool SURF>
+template <bool JET, int SURF>
 cudaError_t launch_trace_t(const TraceLaunch& L, cudaStream_t stream) {
     if (L.precision == BH_PRECISION_MIXED) {
         cudaError_t e;
@@ -1329,8 +1339,10 @@ cudaError_t launch_eval_rhs(int precision, const FrameParams* d_frame, const dou
 
 cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
     cudaError_t e;
-    if (L.jet) e = launch_trace_t<true, true>(L, stream);
-    else e = (L.surfaces || L.xing) ? launch_trace_t<false, true>(L, stream) : launch_trace_t<false, false>(L, stream);
+    if (L.jet) e = launch_trace_t<true, kSurfAll>(L, stream);
+    else if (L.surfaces) e = launch_trace_t<false, kSurfAll>(L, stream);
+    else if (L.xing) e = launch_trace_t<false, kSurfCrossings>(L, stream);
+    else e = launch_trace_t<false, kSurfNone>(L, stream);
     if (e != cudaSuccess || !L.band_done) return e;
     // Every band counter up to its band's size once all trace kernels are
     // done (rays a budget or an abort left untraced included), so a stream
@@ -1341,10 +1353,10 @@ cudaError_t launch_trace(const TraceLaunch& L, cudaStream_t stream) {
 }
 
 int trace_blocks_per_sm(int precision, int block_size, int variant) {
-    const void* k[3];
+    const void* k[kFamily];
     kernels_of(precision, variant, k);
     int least = 0;
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < kFamily; ++i) {
         int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k[i], block_size, 0);
         if (i == 0 || n < least) least = n;
@@ -1353,10 +1365,10 @@ int trace_blocks_per_sm(int precision, int block_size, int variant) {
 }
 
 int trace_registers(int precision, int variant) {
-    const void* k[3];
+    const void* k[kFamily];
     kernels_of(precision, variant, k);
     int most = 0;
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < kFamily; ++i) {
         cudaFuncAttributes at;
         cudaFuncGetAttributes(&at, k[i]);
         if (at.numRegs > most) most = at.numRegs;
