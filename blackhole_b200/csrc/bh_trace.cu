@@ -155,7 +155,6 @@ struct Lane {
     int att0;                // attempts already counted against the budget
     double jet;              // jet emission picked up so far (jet kernels only)
     int gid, frame;
-    int have_k1;
     int mirror;              // mixed: the state holds pi - th and -p_th
     int factored;
     int bad_sc;
@@ -518,7 +517,6 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     L.factored = F.factored_delta;
     L.bad_sc = (F.atol + F.rtol * fabs(y8[4]) == 0.0) || (F.atol + F.rtol * fabs(y8[7]) == 0.0);
     L.tries = 0;
-    L.have_k1 = 0;
     if (JET) L.jet = A.resume ? A.jet[L.gid] : 0.0;
     // p_t and p_phi never change: store them now, the rest at termination.
     A.hits[L.gid].y[4] = y8[4];
@@ -559,8 +557,8 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
     L.inv_Q0 = (float)(1.0 / (fabs(L.Q0) + 1e-12));
     L.mirror = 0;
     if (P::kMixed && F.mirror_ok && !dr && (double)L.y[2] > 0.5 * kPi) {
-        // a camera below the equator: start in the mirror image (the first
-        // attempt evaluates k1 and cos(th) there)
+        // a camera below the equator: start in the mirror image (k1 and
+        // cos(th) are evaluated there, below)
         L.y[2] = (R)((kPiHi - (float)L.y[2]) + kPiLo);
         L.y[5] = -L.y[5];
         L.mirror = 1;
@@ -569,6 +567,19 @@ __device__ bool start_ray(const TraceArgs& A, Lane<P>& L, long long id) {
         write_hit<P, JET>(A, L, BH_HIT_EXHAUSTED, y8);
         return false;
     }
+    // The first stage (FSAL: every later step starts from the last one's
+    // stage 7) and the base angle's sin/cos, here rather than behind a branch
+    // in the step loop (-2.3% per mixed frame, -1.4% per FP64 frame).
+    Aux<P> ax;
+    if constexpr (P::kMixed) {
+        rhs<P>(L, L.y[1], L.y[2], L.y[4], L.y[5], L.k1, &ax);
+    } else {
+        double sn, cs;
+        stage_sincos_far<P>(L.y[2], &sn, &cs);
+        rhs_sc<P>(L, L.y[1], sn, cs, L.y[4], L.y[5], L.k1, &ax);
+    }
+    L.c0 = ax.cs;
+    L.sn0 = ax.sn;
     return true;
 }
 
@@ -596,20 +607,6 @@ __device__ bool attempt(const TraceArgs& A, Lane<P>& L) {
             const double hmax = F.hmax_a * dmaxr(1.0, L.y[1] - F.r_h) + F.hmax_b;
             if (L.h > hmax) L.h = hmax;
         }
-    }
-    if (!L.have_k1) {
-        Aux<P> ax;
-        if constexpr (P::kMixed) {
-            rhs<P>(L, L.y[1], L.y[2], L.y[4], L.y[5], L.k1, &ax);
-        } else {
-            // binary64: no full sin/cos inline in the step loop (below)
-            double sn, cs;
-            stage_sincos_far<P>(L.y[2], &sn, &cs);
-            rhs_sc<P>(L, L.y[1], sn, cs, L.y[4], L.y[5], L.k1, &ax);
-        }
-        L.c0 = ax.cs;
-        L.sn0 = ax.sn;
-        L.have_k1 = 1;
     }
     if (L.tries == 0 && F.land_escape && L.k1[1] > typename P::R(0) &&
         (float)L.y[1] + (float)L.h * (float)L.k1[1] > F.f_land_limit && (double)L.y[1] < F.r_escape) {
